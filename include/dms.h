@@ -1,0 +1,237 @@
+/*
+ * dms.h — C ABI of the B200 trajectory engine (libdms_cuda.so).
+ *
+ * The engine replaces the per-trajectory Monte Carlo of DaMaSCUS-SUN-EVAP and the MPI batching
+ * that drives it.  Reference interfaces replaced, by entry point:
+ *   dms_load_solar_model   Solar_Model::Solar_Model()                include/Solar_Model.hpp:320,
+ *                                                                    src/Solar_Model.cpp:128-166
+ *   dms_add_point          DM particle construction + Solar_Model::Interpolate_Total_DM_Scattering_Rate
+ *                                                                    src/Parameter_Scan.cpp:386-471,
+ *                                                                    include/Solar_Model.hpp:338
+ *   dms_run                Simulation_Data::Generate_Data trajectory loop (simulate_one_trajectory
+ *                          + MPI rounds/tail work)                  include/Data_Generation.hpp:134,
+ *                                                                    src/Data_Generation.cpp:488-972
+ *   dms_run_records        Initial_Conditions + Hyperbolic_Kepler_Shift + Trajectory_Simulator::Simulate
+ *                          for listed trajectories                   include/Simulation_Trajectory.hpp:174
+ *   dms_get_results        Simulation_Data accumulators after Perform_MPI_Reductions
+ *                                                                    src/Data_Generation.cpp:974-1210
+ *   dms_rate               Solar_Model::Total_DM_Scattering_Rate     include/Solar_Model.hpp:334
+ *
+ * Conventions: every call returns DMS_OK (0) or a negative DMS_ERR_* code, and the message of
+ * the last failure is available from dms_last_error().  No C++ exception crosses the ABI.
+ * Pointers passed in are caller-owned and only read during the call (copied where kept).
+ * One host thread per context; contexts on different devices may coexist.
+ * Units: km, s, km/s, eV, K; cross sections in cm^2 and masses in GeV at the boundary.
+ */
+#ifndef DMS_H
+#define DMS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+#define DMS_OK                    0
+#define DMS_ERR_INVALID_ARGUMENT (-1)
+#define DMS_ERR_CUDA             (-2)
+#define DMS_ERR_IO               (-3)
+#define DMS_ERR_NO_SOLAR_MODEL   (-4)
+#define DMS_ERR_NO_POINT         (-5)
+#define DMS_ERR_CAPACITY         (-6)
+#define DMS_ERR_BUDGET           (-7)
+#define DMS_ERR_CANCELLED        (-8)
+#define DMS_ERR_STATE            (-9)
+
+/* ---- termination reasons: TrajectoryTerminationReason, include/Simulation_Trajectory.hpp:35-48 */
+#define DMS_REASON_UNKNOWN              0
+#define DMS_REASON_OUTWARD_ESCAPE       1
+#define DMS_REASON_SCATTER              2
+#define DMS_REASON_WALL_TIME_LIMIT      3
+#define DMS_REASON_MAX_FREE_STEPS       4
+#define DMS_REASON_MAX_SCATTERINGS      5
+#define DMS_REASON_NON_FINITE_STATE     6
+#define DMS_REASON_SPEED_LIMIT          7
+#define DMS_REASON_NUMERICAL_FAILURE    8
+#define DMS_REASON_CAPTURE_MODE         9
+#define DMS_REASON_ENERGY_DRIFT_ESCAPE 10
+#define DMS_REASON_COUNT               11
+
+/* record flags */
+#define DMS_REC_SHIFT_OK          0x01u   /* initial Hyperbolic_Kepler_Shift succeeded */
+#define DMS_REC_CAPTURED          0x02u   /* TrajectoryBincount::is_captured */
+#define DMS_REC_EVENT_OBSERVED    0x04u
+#define DMS_REC_SURVIVAL_VALID    0x08u
+#define DMS_REC_BOUNDARY_ESCAPE   0x10u
+#define DMS_REC_FREE              0x20u   /* Trajectory_Result::Particle_Free */
+#define DMS_REC_REFLECTED         0x40u   /* Trajectory_Result::Particle_Reflected */
+#define DMS_REC_REFLECT_SHIFT_OK  0x80u   /* final Kepler shift to 1 AU succeeded (reflected only) */
+#define DMS_REC_INVALID_ESCAPE    0x100u  /* numerically_invalid_escape */
+
+/* Per-trajectory outcome (Trajectory_Result + TrajectoryBincount scalars,
+ * include/Simulation_Trajectory.hpp:53-85, 101-114).  Times in s, positions in km,
+ * velocities in km/s.  The same layout is produced by the engine, the CPU oracle and the
+ * reference build of the oracle. */
+typedef struct
+{
+	uint64_t trajectory_id;
+	uint64_t number_of_scatterings;
+	uint64_t number_of_draws;          /* uniform draws consumed (replay check) */
+	uint32_t point;
+	uint32_t termination_reason;       /* DMS_REASON_* */
+	uint32_t flags;                    /* DMS_REC_* */
+	uint32_t reserved;
+	double initial_time;               /* event after the initial Kepler shift */
+	double initial_position[3];
+	double initial_velocity[3];
+	double final_time;
+	double final_position[3];
+	double final_velocity[3];
+	double t_capture;                  /* -1 if never captured */
+	double t_last_bound;
+	double t_final_unbinding_scatter;  /* NaN if none */
+	double t_boundary_escape;          /* NaN if none */
+	double t_termination;
+	double max_free_energy_drift_eV;
+	double max_free_energy_drift_rel;
+	double lifetime_unbinding;         /* t_final_unbinding - t_capture for completed events, else -1 */
+} dms_traj_record;
+
+/* ---- context ----------------------------------------------------------------------------- */
+typedef struct dms_ctx dms_ctx;
+
+int dms_create(dms_ctx** ctx, int device);
+void dms_destroy(dms_ctx* ctx);
+const char* dms_last_error(const dms_ctx* ctx);
+/* Request cancellation of a running dms_run from another host thread (mapped flag). */
+int dms_cancel(dms_ctx* ctx);
+
+/* ---- solar model ------------------------------------------------------------------------- */
+/* Loads the AGSS09 table (35 columns, 20 header lines) and builds the radial tables on the
+ * device: G*M(r), T(r), v_esc^2(r), n_e(r) and n_i(r) for the 63 isotope targets. */
+int dms_load_solar_model(dms_ctx* ctx, const char* path);
+
+/* ---- parameter points -------------------------------------------------------------------- */
+typedef struct
+{
+	double mass_gev;                   /* DM_mass */
+	double sigma_p_cm2;                /* DM_cross_section_nucleon (SI contact, low-mass mode) */
+	double sigma_e_cm2;                /* DM_cross_section_electron */
+	double fn_over_fp;                 /* 1.0 when DM_isospin_conserved */
+	double halo_v0_kms;                /* SHM_v0 */
+	double halo_vesc_kms;              /* SHM_vEscape */
+	double halo_vobs_kms[3];           /* SHM_vObserver */
+	uint32_t interpolation_points;     /* N of the N x N total-rate grid; must be >= 2 */
+	uint32_t reserved;
+} dms_point_params;
+
+/* Adds a parameter point and builds its N x N total-rate grid on the device (one kernel,
+ * Total_DM_Scattering_Rate_Computed at every node, src/Solar_Model.cpp:395-465). */
+int dms_add_point(dms_ctx* ctx, const dms_point_params* params, int* point_id);
+int dms_num_points(const dms_ctx* ctx);
+
+/* Scattering rate [1/s] of point `point_id` at radius r_km and speed v_kms, through the
+ * interpolated grid (interpolated = 1) or the direct sum over targets (interpolated = 0).
+ * Evaluated on the device for n query pairs. */
+int dms_rate(dms_ctx* ctx, int point_id, int interpolated, const double* r_km, const double* v_kms, double* rate_out, size_t n);
+
+/* ---- runs -------------------------------------------------------------------------------- */
+#define DMS_PRECISION_FP64  0
+
+typedef struct
+{
+	uint32_t seed;                     /* fixed_seed; draw-stream key */
+	int32_t capture_mode;              /* 1: stop each trajectory at the first post-scatter E < 0 */
+	uint64_t max_scatterings;          /* maximum_number_of_scatterings */
+	uint64_t max_free_steps;           /* maximum_free_time_steps */
+	double boundary_radius_rsun;       /* initial_and_final_radius / R_sun (2.0) */
+	int32_t precision;                 /* DMS_PRECISION_* */
+	uint32_t threads_per_block;        /* 0 = default */
+	uint32_t blocks_per_sm;            /* 0 = default */
+	uint32_t queue_chunk;              /* trajectories claimed per queue fetch; 0 = default */
+	uint64_t iteration_budget;         /* per-lane loop-iteration bound; 0 = default */
+} dms_run_opts;
+
+typedef struct
+{
+	int32_t point_id;
+	uint32_t reserved;
+	uint64_t first_trajectory;         /* trajectory ids [first, first + count) */
+	uint64_t count;
+} dms_work_range;
+
+void dms_default_run_opts(dms_run_opts* opts);
+
+/* Simulates every trajectory of the given ranges in one persistent launch and adds the
+ * outcomes to the per-point accumulators (counters, the four 2000-bin histograms with their
+ * per-trajectory sums of squares, completed evaporation events). */
+int dms_run(dms_ctx* ctx, const dms_run_opts* opts, const dms_work_range* ranges, int n_ranges);
+
+/* Simulates trajectories [first, first + count) of one point and returns one record per
+ * trajectory (host buffer of `count` records).  Does not touch the accumulators.  When
+ * hist_dt / hist_v2dt are non-null they receive each trajectory's own 2000-bin
+ * histograms (count * 2000 doubles each). */
+int dms_run_records(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64_t first, uint64_t count,
+                    dms_traj_record* records, double* hist_dt, double* hist_v2dt);
+
+/* ---- results ----------------------------------------------------------------------------- */
+/* Counter slots of dms_point_results.counters (Simulation_Data members,
+ * include/Data_Generation.hpp:78-95). */
+#define DMS_CNT_TRAJECTORIES              0
+#define DMS_CNT_FREE                      1
+#define DMS_CNT_REFLECTED                 2
+#define DMS_CNT_CAPTURED                  3
+#define DMS_CNT_COMPLETED_OUTWARD         4
+#define DMS_CNT_COMPLETE_EVAPORATION      5
+#define DMS_CNT_CENSORED_CAPTURED         6
+#define DMS_CNT_INVALID_SURVIVAL          7
+#define DMS_CNT_INITIAL_SHIFT_FAILURES    8
+#define DMS_CNT_FINAL_REFLECTION_SHIFT_FAILURES 9
+#define DMS_CNT_NUMERICAL_FAILURES        10
+#define DMS_CNT_COMPUTATIONAL_TRUNCATIONS 11
+#define DMS_CNT_TOTAL_SCATTERINGS         12
+#define DMS_CNT_RK_STEPS                  13   /* accepted free-propagation steps (work counter) */
+#define DMS_CNT_EVENTS_DROPPED            14   /* evaporation events beyond the buffer capacity */
+#define DMS_CNT_REASON_BASE               16   /* + DMS_REASON_*: trajectories per termination reason */
+#define DMS_NUM_COUNTERS                  32
+
+/* Histogram slots (each DMS_NUM_BINS doubles), src/Data_Generation.cpp:101-110 */
+#define DMS_HIST_CAPTURED_DT         0
+#define DMS_HIST_CAPTURED_V2DT       1
+#define DMS_HIST_NOT_CAPTURED_DT     2
+#define DMS_HIST_NOT_CAPTURED_V2DT   3
+#define DMS_HIST_CAPTURED_DT_SQ      4
+#define DMS_HIST_CAPTURED_V2DT_SQ    5
+#define DMS_HIST_NOT_CAPTURED_DT_SQ  6
+#define DMS_HIST_NOT_CAPTURED_V2DT_SQ 7
+#define DMS_NUM_HISTS                8
+
+/* CompactEvaporationEvent, include/Data_Generation.hpp:48-54 */
+typedef struct
+{
+	uint64_t trajectory_id;
+	double lifetime_unbinding;
+} dms_evaporation_event;
+
+typedef struct
+{
+	uint64_t counters[DMS_NUM_COUNTERS];
+	double* histograms;                /* caller buffer: DMS_NUM_HISTS * DMS_NUM_BINS doubles, or NULL */
+	dms_evaporation_event* events;     /* caller buffer of events_capacity entries, or NULL */
+	uint64_t events_capacity;
+	uint64_t events_count;             /* events stored on the device (copied: min(count, capacity)) */
+} dms_point_results;
+
+int dms_get_results(dms_ctx* ctx, int point_id, dms_point_results* results);
+int dms_reset_results(dms_ctx* ctx, int point_id);
+
+/* Sizes a caller needs to know. */
+int dms_num_bins(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DMS_H */
