@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Benchmark of the trajectory engine: scatterings/s (and trajectories/s) on B200.
+
+Workload (one "step"): the Parameter-point evaporation configuration -- SI contact,
+m_DM = 0.3 GeV, sigma_n = 1e-36 cm^2, AGSS09, Standard Halo Model (v0 = 220, v_esc = 544,
+v_sun = (11.1, 232.2, 7.3) km/s), 1000 x 1000 rate grid, max 1e6 scatterings, seed 7 -- run
+over one batch of TRAJECTORIES trajectory ids per GPU (enough for the 8192 captured particles
+of the configuration's sample_size; the captured count of every step is checked).  Each step
+uses fresh trajectory ids.  Inputs are generated on the device from the Philox draw stream, so
+"inputs resident" means the solar tables and rate grid; the per-step host input is the work
+range.  The per-lane histogram scratch (2.4 GB) exceeds L2, and L2 is additionally flushed
+between steps.
+
+Arms:
+  default            the CUDA engine through its C ABI (libdms_cuda.so)
+  --impl reference   the reference's own CPU implementation of the path (oracle/_ref: the
+                     reference sources compiled against restated third-party shims), all host
+                     cores, bounded per-step samples of the same workload
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PACKAGE_DIR = os.path.join(REPO, "damascus-earth-evap_b200")
+sys.path.insert(0, PACKAGE_DIR)
+sys.path.insert(0, os.path.join(REPO, "tests"))
+
+MASS_GEV, SIGMA_CM2, GRID_N, SEED, MAX_SCAT = 0.3, 1e-36, 1000, 7, 10 ** 6
+TRAJECTORIES = 65536
+SAMPLE_SIZE = 8192
+METRIC = "scatterings/s & trajectories/s on 1 B200, batched-FP32 vs plain-FP64 form"
+WORKLOAD = ("Parameter-point evaporation (config 1): SI contact m=0.3 GeV sigma_n=1e-36 cm2, AGSS09, SHM, "
+            "1000x1000 rate grid, max 1e6 scatterings, seed 7; %d trajectories per GPU per step (>= 8192 captures)" % TRAJECTORIES)
+# Algorithmic FP64 operations (add/sub/mul/div/sqrt, one each; transcendental = 1) per unit of
+# work, counted from the source of the path: per RK45 attempt, per accepted free step (event
+# reconstruction, rate lookups, 4-piece optical depth, bincount, energy), per scattering
+# (63-target rate sum, target velocity rejection, kinematics) and per trajectory (initial
+# conditions and Kepler shift).
+FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ = 217.0, 390.0, 2100.0, 800.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------------------------------
+# clocks during the timed region
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------------------------------
+# CPU arm: the reference build (or the C oracle port) in worker processes
+_cpu = {}
+
+
+def _cpu_init(kind):
+    import dms_ctypes
+    if kind == "reference":
+        impl = dms_ctypes.Reference()
+    else:
+        impl = dms_ctypes.Oracle()
+    impl.set_point(dms_ctypes.point_params(MASS_GEV, SIGMA_CM2, interpolation_points=GRID_N))
+    _cpu["impl"] = impl
+
+
+def _cpu_work(task):
+    first_id, seconds, chunk = task
+    impl = _cpu["impl"]
+    t0 = time.perf_counter()
+    ntraj = nscat = ncap = 0
+    nxt = first_id
+    while time.perf_counter() - t0 < seconds:
+        res = impl.run_records(SEED, 0, nxt, chunk, capture_mode=False, max_scatterings=MAX_SCAT)["records"]
+        nxt += chunk
+        ntraj += chunk
+        nscat += sum(r.number_of_scatterings for r in res)
+        ncap += sum(1 for r in res if r.flags & 0x2)
+    return ntraj, nscat, ncap, time.perf_counter() - t0
+
+
+def cpu_kind():
+    import dms_ctypes
+    return "reference" if os.path.exists(dms_ctypes.REF_LIB) else "port"
+
+
+def cpu_pool(cores):
+    kind = cpu_kind()
+    ctx = mp.get_context("spawn")
+    pool = ctx.Pool(cores, initializer=_cpu_init, initargs=(kind,))
+    return pool, kind
+
+
+def cpu_measure(pool, cores, seconds, step):
+    """One bounded sample: every worker runs disjoint trajectory ids for `seconds`."""
+    tasks = [(10 ** 9 + (step * cores + w) * 10 ** 6, seconds, 8) for w in range(cores)]
+    out = pool.map(_cpu_work, tasks)
+    ntraj = sum(o[0] for o in out)
+    nscat = sum(o[1] for o in out)
+    ncap = sum(o[2] for o in out)
+    wall = max(o[3] for o in out)
+    return ntraj, nscat, ncap, wall
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    seconds = args.reference_step_seconds
+    t_setup = time.perf_counter()
+    pool, kind = cpu_pool(cores)
+    pool.map(_cpu_work, [(0, 0.0, 1)] * cores)  # forces initialisation of every worker
+    log("reference arm: %d workers ready (%s) in %.1fs" % (cores, kind, time.perf_counter() - t_setup))
+    for w in range(args.warmup):
+        cpu_measure(pool, cores, seconds, w)
+    tot_traj = tot_scat = tot_cap = 0
+    tot_time = 0.0
+    for s in range(args.steps):
+        ntraj, nscat, ncap, wall = cpu_measure(pool, cores, seconds, args.warmup + s)
+        tot_traj += ntraj
+        tot_scat += nscat
+        tot_cap += ncap
+        tot_time += wall
+    pool.close()
+    pool.join()
+    value = tot_scat / tot_time
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "scatterings/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_time / max(args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "trajectories_per_s": tot_traj / tot_time, "captured_per_s": tot_cap / tot_time,
+        "config": {"workload": WORKLOAD.replace("%d trajectories per GPU per step" % TRAJECTORIES,
+                                                "bounded %.0f s sample per worker per step" % seconds),
+                   "mass_gev": MASS_GEV, "sigma_cm2": SIGMA_CM2, "seed": SEED, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "scatterings/s", "cores": cores, "kind": kind,
+                         "sample": "%d x %.0f s per step, %d trajectories in total" % (cores, seconds, tot_traj)},
+        "e2e": {"value": value, "unit": "scatterings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------
+# engine arm
+def run_engine_arm(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    import torch.distributed as dist
+
+    pool = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # spawn the CPU workers before the first GPU call
+        pool, kind = cpu_pool(os.cpu_count() or 1)
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local_rank),
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    import dms_b200
+    engine = dms_b200.Engine(local_rank)
+    pid = engine.add_point(dms_b200.point_params(MASS_GEV, SIGMA_CM2, interpolation_points=GRID_N))
+    opts = dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT, time_limit_s=600.0)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    peak = engine.fp64_peak_tflops()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def ids(step):
+        return (step * world + rank) * TRAJECTORIES
+
+    # warm-up
+    for w in range(args.warmup):
+        engine.reset_results(pid)
+        engine.run([(pid, ids(w), TRAJECTORIES)], opts)
+        flush.zero_()
+    # timed region: device time of the trajectory launches
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    barrier()
+    dev_ms = 0.0
+    tot = {"trajectories": 0, "total_scatterings": 0, "captured": 0, "rk_steps": 0, "rk_attempts": 0}
+    min_captured = None
+    for s in range(args.steps):
+        engine.reset_results(pid)
+        engine.run([(pid, ids(args.warmup + s), TRAJECTORIES)], opts)
+        dev_ms += engine.last_kernel_ms()
+        c = engine.results(pid, events_capacity=1)["counters"]
+        for k in tot:
+            tot[k] += c[k]
+        min_captured = c["captured"] if min_captured is None else min(min_captured, c["captured"])
+        flush.zero_()
+    barrier()
+    clock_info = clocks.stop()
+    # e2e: through the C ABI with host buffers; every step copies its work range in and its
+    # counters, histograms and evaporation events out
+    barrier()
+    t0 = time.perf_counter()
+    e2e_scat = 0
+    d2h_bytes = 0
+    for s in range(args.steps):
+        engine.reset_results(pid)
+        engine.run([(pid, ids(args.warmup + args.steps + s), TRAJECTORIES)], opts)
+        res = engine.results(pid, events_capacity=1 << 16)
+        e2e_scat += res["counters"]["total_scatterings"]
+        d2h_bytes += 8 * 32 + res["histograms"].nbytes + 16 * len(res["events"])
+    barrier()
+    e2e_s = time.perf_counter() - t0
+
+    totals = torch.tensor([float(tot["total_scatterings"]), float(tot["trajectories"]), float(e2e_scat)],
+                          dtype=torch.float64, device="cuda")
+    times = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(totals, op=dist.ReduceOp.SUM)
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    dev_s = float(times[0]) * 1e-3
+    value = float(totals[0]) / dev_s
+    traj_rate = float(totals[1]) / dev_s
+    e2e_value = float(totals[2]) / float(times[1])
+    flops = (FLOP_PER_ATTEMPT * tot["rk_attempts"] + FLOP_PER_STEP * tot["rk_steps"] +
+             FLOP_PER_SCATTER * tot["total_scatterings"] + FLOP_PER_TRAJ * tot["trajectories"])
+    achieved = flops / (dev_ms * 1e-3) / 1e12
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "scatterings/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "trajectories_per_s": traj_rate,
+            "captured_per_step_min": min_captured,
+            "config": {"workload": WORKLOAD, "mass_gev": MASS_GEV, "sigma_cm2": SIGMA_CM2, "grid": GRID_N,
+                       "trajectories_per_gpu_step": TRAJECTORIES, "seed": SEED, "precision": "fp64 (no FMA contraction)",
+                       "parallelism": "trajectory ids sharded over %d GPU(s), no data-path collective" % world,
+                       "l2": "per-lane histogram scratch > L2, plus 256 MB flush between steps"},
+            "e2e": {"value": e2e_value, "unit": "scatterings/s", "h2d_bytes_per_step": 64,
+                    "d2h_bytes_per_step": int(d2h_bytes / max(args.steps, 1))},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                         "peak_source": "measured in this run: DFMA-chain kernel on all SMs (2 FLOP per FMA)",
+                         "flop_model": "%.0f/attempt + %.0f/step + %.0f/scattering + %.0f/trajectory" % (
+                             FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ)},
+            "clocks": clock_info,
+        }
+    engine.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        if pool is not None:
+            ntraj, nscat, ncap, wall = cpu_measure(pool, os.cpu_count() or 1, args.cpu_baseline_seconds, 0)
+            pool.close()
+            pool.join()
+            line["cpu_baseline"] = {"value": nscat / wall, "unit": "scatterings/s", "cores": os.cpu_count() or 1,
+                                    "kind": cpu_kind(),
+                                    "sample": "%d trajectories of the same point, %.0f s on every core" % (
+                                        ntraj, args.cpu_baseline_seconds)}
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-baseline-seconds", type=float, default=12.0)
+    ap.add_argument("--reference-step-seconds", type=float, default=6.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_engine_arm(args)
+
+
+if __name__ == "__main__":
+    main()

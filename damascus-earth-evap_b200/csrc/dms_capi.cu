@@ -1,0 +1,693 @@
+// C ABI of the trajectory engine (include/dms.h): context, device memory, launches.
+//
+// Device memory layout of a context (all FP64 unless noted):
+//   radial tables   one allocation: r, G*M, T, v_esc^2, n_e (+ slopes) and the 63 isotope densities
+//                   node-major (+ slopes), and the uint16 bucket index of the knot search
+//   points          DevPoint[capacity] (constants of every parameter point) and one N x N rate
+//                   grid per point (radius-major, as the reference's rate_grid)
+//   accumulators    counters [points x 32] u64, histograms [points x 8 x 2000], evaporation
+//                   events [points x event capacity]
+//   lane scratch    one 2000-bin (dt, v2dt) row per resident lane; zero between trajectories
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/dms.h"
+#include "dms_host_model.h"
+#include "dms_kernels.cuh"
+
+using namespace dms;
+
+struct dms_ctx
+{
+	int device = 0;
+	int sm_count = 0;
+	std::string error;
+	cudaStream_t stream = nullptr;
+	// solar model
+	bool has_solar = false;
+	SolarTables tables;
+	void* d_tables = nullptr;
+	DevSolar dsolar{};
+	// points
+	std::vector<PointConstants> points;
+	std::vector<double*> d_grids;
+	DevPoint* d_points = nullptr;
+	int point_capacity = 0;
+	// accumulators
+	unsigned long long* d_counters = nullptr;
+	double* d_hists = nullptr;
+	dms_evaporation_event* d_events = nullptr;
+	unsigned long long* d_event_count = nullptr;
+	uint64_t event_capacity = 1ULL << 20;
+	// run scratch
+	double2* d_lane_hist = nullptr;
+	size_t lane_capacity = 0;
+	unsigned long long* d_queue = nullptr;
+	unsigned int* d_status = nullptr;
+	int* h_cancel = nullptr;       // mapped host memory
+	int* d_cancel = nullptr;
+	cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+	double last_kernel_ms = 0.0;
+};
+
+namespace
+{
+int Fail(dms_ctx* ctx, int code, const std::string& msg)
+{
+	if(ctx)
+		ctx->error = msg;
+	return code;
+}
+
+#define DMS_CUDA(ctx, call)                                                                                   \
+	do                                                                                                        \
+	{                                                                                                         \
+		const cudaError_t e_ = (call);                                                                        \
+		if(e_ != cudaSuccess)                                                                                 \
+			return Fail(ctx, DMS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));             \
+	} while(0)
+
+constexpr int MAX_POINTS = 4096;
+
+int Grow_Points(dms_ctx* ctx, int needed)
+{
+	if(needed <= ctx->point_capacity)
+		return DMS_OK;
+	int cap = std::max(8, ctx->point_capacity);
+	while(cap < needed) cap *= 2;
+	DevPoint* np = nullptr;
+	unsigned long long* nc = nullptr;
+	double* nh = nullptr;
+	dms_evaporation_event* ne = nullptr;
+	unsigned long long* nn = nullptr;
+	DMS_CUDA(ctx, cudaMalloc(&np, sizeof(DevPoint) * cap));
+	DMS_CUDA(ctx, cudaMalloc(&nc, sizeof(unsigned long long) * DMS_NUM_COUNTERS * cap));
+	DMS_CUDA(ctx, cudaMalloc(&nh, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS * cap));
+	DMS_CUDA(ctx, cudaMalloc(&ne, sizeof(dms_evaporation_event) * ctx->event_capacity * cap));
+	DMS_CUDA(ctx, cudaMalloc(&nn, sizeof(unsigned long long) * cap));
+	DMS_CUDA(ctx, cudaMemset(nc, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS * cap));
+	DMS_CUDA(ctx, cudaMemset(nh, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS * cap));
+	DMS_CUDA(ctx, cudaMemset(nn, 0, sizeof(unsigned long long) * cap));
+	const int old = static_cast<int>(ctx->points.size());
+	if(old > 0)
+	{
+		DMS_CUDA(ctx, cudaMemcpy(np, ctx->d_points, sizeof(DevPoint) * old, cudaMemcpyDeviceToDevice));
+		DMS_CUDA(ctx, cudaMemcpy(nc, ctx->d_counters, sizeof(unsigned long long) * DMS_NUM_COUNTERS * old, cudaMemcpyDeviceToDevice));
+		DMS_CUDA(ctx, cudaMemcpy(nh, ctx->d_hists, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS * old, cudaMemcpyDeviceToDevice));
+		for(int p = 0; p < old; p++)
+			DMS_CUDA(ctx, cudaMemcpy(ne + p * ctx->event_capacity, ctx->d_events + p * ctx->event_capacity,
+			                         sizeof(dms_evaporation_event) * ctx->event_capacity, cudaMemcpyDeviceToDevice));
+		DMS_CUDA(ctx, cudaMemcpy(nn, ctx->d_event_count, sizeof(unsigned long long) * old, cudaMemcpyDeviceToDevice));
+	}
+	cudaFree(ctx->d_points);
+	cudaFree(ctx->d_counters);
+	cudaFree(ctx->d_hists);
+	cudaFree(ctx->d_events);
+	cudaFree(ctx->d_event_count);
+	ctx->d_points = np;
+	ctx->d_counters = nc;
+	ctx->d_hists = nh;
+	ctx->d_events = ne;
+	ctx->d_event_count = nn;
+	ctx->point_capacity = cap;
+	return DMS_OK;
+}
+
+int Ensure_Lanes(dms_ctx* ctx, size_t lanes)
+{
+	if(lanes <= ctx->lane_capacity)
+		return DMS_OK;
+	cudaFree(ctx->d_lane_hist);
+	ctx->d_lane_hist = nullptr;
+	ctx->lane_capacity = 0;
+	DMS_CUDA(ctx, cudaMalloc(&ctx->d_lane_hist, sizeof(double2) * DMS_NUM_BINS * lanes));
+	DMS_CUDA(ctx, cudaMemset(ctx->d_lane_hist, 0, sizeof(double2) * DMS_NUM_BINS * lanes));
+	ctx->lane_capacity = lanes;
+	return DMS_OK;
+}
+
+int Check_Run_Opts(dms_ctx* ctx, const dms_run_opts* o)
+{
+	if(!o)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null run options");
+	if(!(o->boundary_radius_rsun >= 1.0) || !std::isfinite(o->boundary_radius_rsun))
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "boundary radius must be at least one solar radius");
+	if(o->precision != DMS_PRECISION_FP64)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "unsupported precision");
+	if(o->threads_per_block != 0 && (o->threads_per_block % 32 != 0 || o->threads_per_block > 128))
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "threads_per_block must be a multiple of 32 up to 128");
+	return DMS_OK;
+}
+
+// One persistent launch over the given work; polls for completion, enforcing the wall-clock
+// limit through the mapped cancel flag.
+int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
+{
+	const int threads = o->threads_per_block ? static_cast<int>(o->threads_per_block) : 128;
+	const int max_per_sm = Trajectory_Max_Blocks_Per_SM(threads);
+	if(max_per_sm <= 0)
+		return Fail(ctx, DMS_ERR_CUDA, "trajectory kernel cannot be resident with this block size");
+	int per_sm = o->blocks_per_sm ? static_cast<int>(o->blocks_per_sm) : max_per_sm;
+	per_sm = per_sm > max_per_sm ? max_per_sm : per_sm;
+	int blocks = ctx->sm_count * per_sm;
+	const uint64_t needed_blocks = (p.total + threads - 1) / threads;
+	if(static_cast<uint64_t>(blocks) > needed_blocks)
+		blocks = static_cast<int>(std::max<uint64_t>(1, needed_blocks));
+	const size_t lanes = static_cast<size_t>(blocks) * threads;
+	int rc = Ensure_Lanes(ctx, lanes);
+	if(rc != DMS_OK)
+		return rc;
+	p.lane_hist = ctx->d_lane_hist;
+	p.queue_head = ctx->d_queue;
+	p.status = ctx->d_status;
+	p.cancel = ctx->d_cancel;
+	p.seed = o->seed;
+	p.capture_mode = o->capture_mode ? 1 : 0;
+	p.max_scatterings = o->max_scatterings;
+	p.max_free_steps = o->max_free_steps;
+	p.boundary = o->boundary_radius_rsun * DMS_RSUN_KM;
+	p.iteration_budget = o->iteration_budget ? o->iteration_budget : ~0ULL;
+	p.ic_max_attempts = 1 << 20;
+	p.S = ctx->dsolar;
+	p.points = ctx->d_points;
+	p.n_points = static_cast<int>(ctx->points.size());
+	*ctx->h_cancel = 0;
+	DMS_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), ctx->stream));
+	DMS_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), ctx->stream));
+	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+	Launch_Trajectories(p, blocks, threads, ctx->stream);
+	DMS_CUDA(ctx, cudaGetLastError());
+	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+	const auto start = std::chrono::steady_clock::now();
+	bool cancelled_by_limit = false;
+	for(;;)
+	{
+		const cudaError_t q = cudaStreamQuery(ctx->stream);
+		if(q == cudaSuccess)
+			break;
+		if(q != cudaErrorNotReady)
+			return Fail(ctx, DMS_ERR_CUDA, std::string("trajectory kernel: ") + cudaGetErrorString(q));
+		if(o->time_limit_s > 0.0 && !cancelled_by_limit)
+		{
+			const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+			if(el > o->time_limit_s)
+			{
+				*reinterpret_cast<volatile int*>(ctx->h_cancel) = 1;
+				cancelled_by_limit = true;
+			}
+		}
+		std::this_thread::sleep_for(std::chrono::microseconds(200));
+	}
+	float kernel_ms = 0.0f;
+	DMS_CUDA(ctx, cudaEventElapsedTime(&kernel_ms, ctx->ev_start, ctx->ev_stop));
+	ctx->last_kernel_ms = kernel_ms;
+	unsigned int status = 0;
+	DMS_CUDA(ctx, cudaMemcpy(&status, ctx->d_status, sizeof status, cudaMemcpyDeviceToHost));
+	if(status & STATUS_CANCELLED)
+		return Fail(ctx, DMS_ERR_CANCELLED, cancelled_by_limit ? "run cancelled: wall-clock limit reached" : "run cancelled");
+	if(status & STATUS_BUDGET)
+		return Fail(ctx, DMS_ERR_BUDGET, "run stopped: per-lane iteration budget exhausted");
+	if(status & STATUS_IC_REJECTION)
+		ctx->error = "warning: an initial-condition rejection loop hit its attempt bound";
+	return DMS_OK;
+}
+
+void Fill_Dev_Point(const PointConstants& c, double* grid, DevPoint& d)
+{
+	std::memset(&d, 0, sizeof d);
+	d.m_dm = c.m_dm;
+	d.sigma_e = c.sigma_e;
+	d.v0 = c.v0;
+	d.vesc_halo = c.vesc_halo;
+	d.vobs = c.vobs;
+	for(int i = 0; i < 3; i++) d.vel_obs[i] = c.vel_obs[i];
+	d.n_esc = c.n_esc;
+	d.avg_speed = c.avg_speed;
+	d.eta0 = c.eta0;
+	d.grid_inv_r = c.grid_inv_r;
+	d.grid_inv_v = c.grid_inv_v;
+	d.grid_vmax = c.grid_vmax;
+	d.grid = grid;
+	d.grid_n = c.grid_n;
+	for(int k = 0; k < DMS_NUM_TARGETS; k++) d.sigma_t[k] = c.sigma_target[k];
+}
+}	// namespace
+
+extern "C" {
+
+int dms_create(dms_ctx** out, int device)
+{
+	if(!out)
+		return DMS_ERR_INVALID_ARGUMENT;
+	*out = nullptr;
+	dms_ctx* ctx = new(std::nothrow) dms_ctx();
+	if(!ctx)
+		return DMS_ERR_CAPACITY;
+	int count = 0;
+	cudaError_t e = cudaGetDeviceCount(&count);
+	if(e != cudaSuccess || device < 0 || device >= count)
+	{
+		delete ctx;
+		return DMS_ERR_CUDA;
+	}
+	ctx->device = device;
+	if(cudaSetDevice(device) != cudaSuccess || cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+	   cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+	   cudaMalloc(&ctx->d_queue, sizeof(unsigned long long)) != cudaSuccess || cudaMalloc(&ctx->d_status, sizeof(unsigned int)) != cudaSuccess ||
+	   cudaHostAlloc(&ctx->h_cancel, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+	   cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->d_cancel), ctx->h_cancel, 0) != cudaSuccess ||
+	   cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev_stop) != cudaSuccess)
+	{
+		dms_destroy(ctx);
+		return DMS_ERR_CUDA;
+	}
+	*ctx->h_cancel = 0;
+	*out = ctx;
+	return DMS_OK;
+}
+
+void dms_destroy(dms_ctx* ctx)
+{
+	if(!ctx)
+		return;
+	cudaSetDevice(ctx->device);
+	if(ctx->stream)
+		cudaStreamSynchronize(ctx->stream);
+	for(double* g : ctx->d_grids) cudaFree(g);
+	cudaFree(ctx->d_tables);
+	cudaFree(ctx->d_points);
+	cudaFree(ctx->d_counters);
+	cudaFree(ctx->d_hists);
+	cudaFree(ctx->d_events);
+	cudaFree(ctx->d_event_count);
+	cudaFree(ctx->d_lane_hist);
+	cudaFree(ctx->d_queue);
+	cudaFree(ctx->d_status);
+	if(ctx->h_cancel)
+		cudaFreeHost(ctx->h_cancel);
+	if(ctx->ev_start)
+		cudaEventDestroy(ctx->ev_start);
+	if(ctx->ev_stop)
+		cudaEventDestroy(ctx->ev_stop);
+	if(ctx->stream)
+		cudaStreamDestroy(ctx->stream);
+	delete ctx;
+}
+
+const char* dms_last_error(const dms_ctx* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+int dms_cancel(dms_ctx* ctx)
+{
+	if(!ctx || !ctx->h_cancel)
+		return DMS_ERR_INVALID_ARGUMENT;
+	*reinterpret_cast<volatile int*>(ctx->h_cancel) = 1;
+	return DMS_OK;
+}
+
+int dms_num_bins(void) { return DMS_NUM_BINS; }
+
+int dms_measure_fp64_peak(dms_ctx* ctx, double* tflops)
+{
+	if(!ctx || !tflops)
+		return DMS_ERR_INVALID_ARGUMENT;
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	const double t = Measure_FP64_Peak(ctx->sm_count, ctx->stream);
+	if(!(t > 0.0))
+		return Fail(ctx, DMS_ERR_CUDA, "FP64 peak probe failed");
+	*tflops = t;
+	return DMS_OK;
+}
+
+int dms_last_kernel_ms(const dms_ctx* ctx, double* ms)
+{
+	if(!ctx || !ms)
+		return DMS_ERR_INVALID_ARGUMENT;
+	*ms = ctx->last_kernel_ms;
+	return DMS_OK;
+}
+
+int dms_load_solar_model(dms_ctx* ctx, const char* path)
+{
+	if(!ctx || !path)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	SolarTables t;
+	const std::string err = Load_Solar_Tables(path, t);
+	if(!err.empty())
+		return Fail(ctx, DMS_ERR_IO, err);
+	const size_t n = t.n, nt = static_cast<size_t>(t.n) * DMS_NUM_TARGETS;
+	const size_t doubles = 9 * n + 2 * nt + DMS_NUM_TARGETS;
+	const size_t bytes = doubles * sizeof(double) + sizeof(uint16_t) * t.bucket_index.size();
+	std::vector<char> host(bytes);
+	double* h = reinterpret_cast<double*>(host.data());
+	const std::vector<double>* parts[11] = {&t.r, &t.gm, &t.gm_s, &t.temp, &t.temp_s, &t.vesc2, &t.vesc2_s, &t.ne, &t.ne_s, &t.nt, &t.nt_s};
+	size_t offsets[11];
+	size_t off = 0;
+	for(int k = 0; k < 11; k++)
+	{
+		offsets[k] = off;
+		std::memcpy(h + off, parts[k]->data(), parts[k]->size() * sizeof(double));
+		off += parts[k]->size();
+	}
+	const size_t off_mass = off;
+	std::memcpy(h + off, t.target_mass_gev, sizeof(double) * DMS_NUM_TARGETS);
+	off += DMS_NUM_TARGETS;
+	std::memcpy(h + off, t.bucket_index.data(), sizeof(uint16_t) * t.bucket_index.size());
+	void* d = nullptr;
+	DMS_CUDA(ctx, cudaMalloc(&d, bytes));
+	const cudaError_t ce = cudaMemcpy(d, host.data(), bytes, cudaMemcpyHostToDevice);
+	if(ce != cudaSuccess)
+	{
+		cudaFree(d);
+		return Fail(ctx, DMS_ERR_CUDA, std::string("table upload: ") + cudaGetErrorString(ce));
+	}
+	cudaFree(ctx->d_tables);
+	ctx->d_tables = d;
+	const double* dd = reinterpret_cast<const double*>(d);
+	DevSolar& S = ctx->dsolar;
+	S.n = t.n;
+	S.nbuckets = t.nbuckets;
+	S.bucket_scale = static_cast<double>(t.nbuckets) / DMS_RSUN_KM;
+	S.r = dd + offsets[0];
+	S.gm = dd + offsets[1];
+	S.gm_s = dd + offsets[2];
+	S.temp = dd + offsets[3];
+	S.temp_s = dd + offsets[4];
+	S.vesc2 = dd + offsets[5];
+	S.vesc2_s = dd + offsets[6];
+	S.ne = dd + offsets[7];
+	S.ne_s = dd + offsets[8];
+	S.nt = dd + offsets[9];
+	S.nt_s = dd + offsets[10];
+	S.target_mass = dd + off_mass;
+	S.bucket = reinterpret_cast<const uint16_t*>(dd + off);
+	ctx->tables = std::move(t);
+	ctx->has_solar = true;
+	return DMS_OK;
+}
+
+int dms_solar_table(dms_ctx* ctx, int which, double* out, size_t capacity)
+{
+	if(!ctx)
+		return DMS_ERR_INVALID_ARGUMENT;
+	if(!ctx->has_solar)
+		return Fail(ctx, DMS_ERR_NO_SOLAR_MODEL, "no solar model loaded");
+	const DevSolar& S = ctx->dsolar;
+	const double* src = nullptr;
+	size_t n = S.n;
+	switch(which)
+	{
+		case 0: src = S.r; break;
+		case 1: src = S.gm; break;
+		case 2: src = S.temp; break;
+		case 3: src = S.vesc2; break;
+		case 4: src = S.ne; break;
+		case 5:
+			src = S.nt;
+			n = static_cast<size_t>(S.n) * DMS_NUM_TARGETS;
+			break;
+		default: return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "unknown table");
+	}
+	if(out)
+	{
+		if(capacity < n)
+			return Fail(ctx, DMS_ERR_CAPACITY, "output buffer too small");
+		DMS_CUDA(ctx, cudaMemcpy(out, src, n * sizeof(double), cudaMemcpyDeviceToHost));
+	}
+	return static_cast<int>(n);
+}
+
+int dms_add_point(dms_ctx* ctx, const dms_point_params* params, int* point_id)
+{
+	if(!ctx || !params)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	if(!ctx->has_solar)
+		return Fail(ctx, DMS_ERR_NO_SOLAR_MODEL, "load a solar model before adding points");
+	if(static_cast<int>(ctx->points.size()) >= MAX_POINTS)
+		return Fail(ctx, DMS_ERR_CAPACITY, "too many parameter points");
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	PointConstants c;
+	const std::string err = Make_Point_Constants(ctx->tables, *params, c);
+	if(!err.empty())
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, err);
+	const int id = static_cast<int>(ctx->points.size());
+	int rc = Grow_Points(ctx, id + 1);
+	if(rc != DMS_OK)
+		return rc;
+	double* grid = nullptr;
+	DMS_CUDA(ctx, cudaMalloc(&grid, sizeof(double) * c.grid_n * c.grid_n));
+	DevPoint d;
+	Fill_Dev_Point(c, grid, d);
+	const cudaError_t e1 = cudaMemcpy(ctx->d_points + id, &d, sizeof d, cudaMemcpyHostToDevice);
+	if(e1 != cudaSuccess)
+	{
+		cudaFree(grid);
+		return Fail(ctx, DMS_ERR_CUDA, cudaGetErrorString(e1));
+	}
+	Launch_Rate_Grid(ctx->dsolar, ctx->d_points + id, grid, c.grid_n, ctx->stream);
+	const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+	if(e2 != cudaSuccess || cudaGetLastError() != cudaSuccess)
+	{
+		cudaFree(grid);
+		return Fail(ctx, DMS_ERR_CUDA, std::string("rate grid kernel: ") + cudaGetErrorString(e2));
+	}
+	ctx->points.push_back(c);
+	ctx->d_grids.push_back(grid);
+	DMS_CUDA(ctx, cudaMemset(ctx->d_counters + static_cast<size_t>(id) * DMS_NUM_COUNTERS, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS));
+	DMS_CUDA(ctx, cudaMemset(ctx->d_hists + static_cast<size_t>(id) * DMS_NUM_HISTS * DMS_NUM_BINS, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS));
+	DMS_CUDA(ctx, cudaMemset(ctx->d_event_count + id, 0, sizeof(unsigned long long)));
+	if(point_id)
+		*point_id = id;
+	return DMS_OK;
+}
+
+int dms_num_points(const dms_ctx* ctx) { return ctx ? static_cast<int>(ctx->points.size()) : 0; }
+
+int dms_set_rate_grid(dms_ctx* ctx, int point_id, const double* grid, uint32_t n)
+{
+	if(!ctx || !grid)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
+		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	if(static_cast<int>(n) != ctx->points[point_id].grid_n)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "grid size does not match the point's interpolation_points");
+	DMS_CUDA(ctx, cudaMemcpy(ctx->d_grids[point_id], grid, sizeof(double) * n * n, cudaMemcpyHostToDevice));
+	return DMS_OK;
+}
+
+int dms_get_rate_grid(dms_ctx* ctx, int point_id, double* grid, uint32_t n)
+{
+	if(!ctx || !grid)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
+		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	if(static_cast<int>(n) != ctx->points[point_id].grid_n)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "grid size does not match the point's interpolation_points");
+	DMS_CUDA(ctx, cudaMemcpy(grid, ctx->d_grids[point_id], sizeof(double) * n * n, cudaMemcpyDeviceToHost));
+	return DMS_OK;
+}
+
+int dms_rate(dms_ctx* ctx, int point_id, int interpolated, const double* r_km, const double* v_kms, double* rate_out, size_t n)
+{
+	if(!ctx || (n > 0 && (!r_km || !v_kms || !rate_out)))
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
+		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	if(n == 0)
+		return DMS_OK;
+	double* d = nullptr;
+	DMS_CUDA(ctx, cudaMalloc(&d, sizeof(double) * 3 * n));
+	cudaError_t e = cudaMemcpy(d, r_km, sizeof(double) * n, cudaMemcpyHostToDevice);
+	if(e == cudaSuccess)
+		e = cudaMemcpy(d + n, v_kms, sizeof(double) * n, cudaMemcpyHostToDevice);
+	if(e == cudaSuccess)
+	{
+		Launch_Rate_Query(ctx->dsolar, ctx->d_points + point_id, interpolated, d, d + n, d + 2 * n, n, ctx->stream);
+		e = cudaStreamSynchronize(ctx->stream);
+	}
+	if(e == cudaSuccess)
+		e = cudaMemcpy(rate_out, d + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+	cudaFree(d);
+	if(e != cudaSuccess)
+		return Fail(ctx, DMS_ERR_CUDA, std::string("rate query: ") + cudaGetErrorString(e));
+	return DMS_OK;
+}
+
+void dms_default_run_opts(dms_run_opts* o)
+{
+	if(!o)
+		return;
+	std::memset(o, 0, sizeof *o);
+	o->seed = 1;
+	o->capture_mode = 0;
+	o->max_scatterings = 100000000000000ULL;   // DEFAULT_MAXIMUM_SCATTERINGS
+	o->max_free_steps = 1000000000000ULL;      // DEFAULT_MAXIMUM_FREE_TIME_STEPS
+	o->boundary_radius_rsun = 2.0;
+	o->precision = DMS_PRECISION_FP64;
+}
+
+int dms_run(dms_ctx* ctx, const dms_run_opts* opts, const dms_work_range* ranges, int n_ranges)
+{
+	if(!ctx)
+		return DMS_ERR_INVALID_ARGUMENT;
+	int rc = Check_Run_Opts(ctx, opts);
+	if(rc != DMS_OK)
+		return rc;
+	if(n_ranges <= 0 || !ranges)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "no work ranges");
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	std::vector<int32_t> pts(n_ranges);
+	std::vector<uint64_t> firsts(n_ranges), offsets(n_ranges + 1);
+	uint64_t total = 0;
+	for(int k = 0; k < n_ranges; k++)
+	{
+		if(ranges[k].point_id < 0 || ranges[k].point_id >= static_cast<int>(ctx->points.size()))
+			return Fail(ctx, DMS_ERR_NO_POINT, "work range names an unknown point");
+		pts[k] = ranges[k].point_id;
+		firsts[k] = ranges[k].first_trajectory;
+		offsets[k] = total;
+		total += ranges[k].count;
+	}
+	offsets[n_ranges] = total;
+	if(total == 0)
+		return DMS_OK;
+	std::vector<char> buf(sizeof(int32_t) * n_ranges + sizeof(uint64_t) * (2 * n_ranges + 1) + 16);
+	void* d = nullptr;
+	DMS_CUDA(ctx, cudaMalloc(&d, buf.size()));
+	char* dc = static_cast<char*>(d);
+	const size_t off_first = 0, off_offset = sizeof(uint64_t) * n_ranges, off_point = sizeof(uint64_t) * (2 * n_ranges + 1);
+	std::memcpy(buf.data() + off_first, firsts.data(), sizeof(uint64_t) * n_ranges);
+	std::memcpy(buf.data() + off_offset, offsets.data(), sizeof(uint64_t) * (n_ranges + 1));
+	std::memcpy(buf.data() + off_point, pts.data(), sizeof(int32_t) * n_ranges);
+	cudaError_t e = cudaMemcpy(d, buf.data(), buf.size(), cudaMemcpyHostToDevice);
+	if(e != cudaSuccess)
+	{
+		cudaFree(d);
+		return Fail(ctx, DMS_ERR_CUDA, cudaGetErrorString(e));
+	}
+	RunParams p{};
+	p.range_first = reinterpret_cast<const uint64_t*>(dc + off_first);
+	p.range_offset = reinterpret_cast<const uint64_t*>(dc + off_offset);
+	p.range_point = reinterpret_cast<const int32_t*>(dc + off_point);
+	p.n_ranges = n_ranges;
+	p.total = total;
+	p.counters = ctx->d_counters;
+	p.hists = ctx->d_hists;
+	p.events = ctx->d_events;
+	p.event_count = ctx->d_event_count;
+	p.event_capacity = ctx->event_capacity;
+	rc = Launch_And_Wait(ctx, opts, p);
+	cudaFree(d);
+	return rc;
+}
+
+int dms_run_records(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64_t first, uint64_t count, dms_traj_record* records,
+                    double* hist_dt, double* hist_v2dt)
+{
+	if(!ctx)
+		return DMS_ERR_INVALID_ARGUMENT;
+	int rc = Check_Run_Opts(ctx, opts);
+	if(rc != DMS_OK)
+		return rc;
+	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
+		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	if(count == 0)
+		return DMS_OK;
+	if(!records || ((hist_dt == nullptr) != (hist_v2dt == nullptr)))
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "records buffer required; histograms need both buffers");
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	const bool want_hist = hist_dt != nullptr;
+	const size_t hist_bytes = want_hist ? sizeof(double) * DMS_NUM_BINS * count : 0;
+	const size_t rec_bytes = sizeof(dms_traj_record) * count;
+	const size_t meta = 64;
+	char* d = nullptr;
+	DMS_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&d), meta + rec_bytes + 2 * hist_bytes));
+	struct Meta
+	{
+		uint64_t first, off0, off1;
+		int32_t point;
+	} m{first, 0, count, point_id};
+	cudaError_t e = cudaMemcpy(d, &m, sizeof m, cudaMemcpyHostToDevice);
+	if(e == cudaSuccess)
+		e = cudaMemset(d + meta, 0, rec_bytes + 2 * hist_bytes);
+	if(e != cudaSuccess)
+	{
+		cudaFree(d);
+		return Fail(ctx, DMS_ERR_CUDA, cudaGetErrorString(e));
+	}
+	RunParams p{};
+	p.range_first = reinterpret_cast<const uint64_t*>(d);
+	p.range_offset = reinterpret_cast<const uint64_t*>(d + 8);
+	p.range_point = reinterpret_cast<const int32_t*>(d + 24);
+	p.n_ranges = 1;
+	p.total = count;
+	p.records = reinterpret_cast<dms_traj_record*>(d + meta);
+	p.rec_hist_dt = want_hist ? reinterpret_cast<double*>(d + meta + rec_bytes) : nullptr;
+	p.rec_hist_v2dt = want_hist ? reinterpret_cast<double*>(d + meta + rec_bytes + hist_bytes) : nullptr;
+	p.counters = ctx->d_counters;
+	p.hists = ctx->d_hists;
+	p.events = ctx->d_events;
+	p.event_count = ctx->d_event_count;
+	p.event_capacity = ctx->event_capacity;
+	rc = Launch_And_Wait(ctx, opts, p);
+	if(rc == DMS_OK || rc == DMS_ERR_CANCELLED || rc == DMS_ERR_BUDGET)
+	{
+		e = cudaMemcpy(records, d + meta, rec_bytes, cudaMemcpyDeviceToHost);
+		if(e == cudaSuccess && want_hist)
+			e = cudaMemcpy(hist_dt, d + meta + rec_bytes, hist_bytes, cudaMemcpyDeviceToHost);
+		if(e == cudaSuccess && want_hist)
+			e = cudaMemcpy(hist_v2dt, d + meta + rec_bytes + hist_bytes, hist_bytes, cudaMemcpyDeviceToHost);
+		if(e != cudaSuccess)
+			rc = Fail(ctx, DMS_ERR_CUDA, cudaGetErrorString(e));
+	}
+	cudaFree(d);
+	return rc;
+}
+
+int dms_get_results(dms_ctx* ctx, int point_id, dms_point_results* r)
+{
+	if(!ctx || !r)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
+		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	DMS_CUDA(ctx, cudaMemcpy(r->counters, ctx->d_counters + static_cast<size_t>(point_id) * DMS_NUM_COUNTERS,
+	                         sizeof(unsigned long long) * DMS_NUM_COUNTERS, cudaMemcpyDeviceToHost));
+	if(r->histograms)
+		DMS_CUDA(ctx, cudaMemcpy(r->histograms, ctx->d_hists + static_cast<size_t>(point_id) * DMS_NUM_HISTS * DMS_NUM_BINS,
+		                         sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS, cudaMemcpyDeviceToHost));
+	unsigned long long count = 0;
+	DMS_CUDA(ctx, cudaMemcpy(&count, ctx->d_event_count + point_id, sizeof count, cudaMemcpyDeviceToHost));
+	r->events_count = std::min<uint64_t>(count, ctx->event_capacity);
+	if(r->events && r->events_capacity > 0)
+	{
+		const uint64_t n = std::min<uint64_t>(r->events_count, r->events_capacity);
+		if(n > 0)
+			DMS_CUDA(ctx, cudaMemcpy(r->events, ctx->d_events + static_cast<size_t>(point_id) * ctx->event_capacity,
+			                         sizeof(dms_evaporation_event) * n, cudaMemcpyDeviceToHost));
+	}
+	return DMS_OK;
+}
+
+int dms_reset_results(dms_ctx* ctx, int point_id)
+{
+	if(!ctx)
+		return DMS_ERR_INVALID_ARGUMENT;
+	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
+		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	DMS_CUDA(ctx, cudaMemset(ctx->d_counters + static_cast<size_t>(point_id) * DMS_NUM_COUNTERS, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS));
+	DMS_CUDA(ctx, cudaMemset(ctx->d_hists + static_cast<size_t>(point_id) * DMS_NUM_HISTS * DMS_NUM_BINS, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS));
+	DMS_CUDA(ctx, cudaMemset(ctx->d_event_count + point_id, 0, sizeof(unsigned long long)));
+	return DMS_OK;
+}
+
+}	// extern "C"

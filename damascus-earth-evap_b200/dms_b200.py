@@ -1,0 +1,242 @@
+"""Python binding of the engine's C ABI (include/dms.h) through ctypes.
+
+The engine is libdms_cuda.so in this directory (built by `make -C damascus-earth-evap_b200`).
+There is no CPU fallback: loading fails loudly when the library or a CUDA device is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY = os.path.join(HERE, "libdms_cuda.so")
+SOLAR_MODEL = os.path.join(HERE, "data", "model_agss09.dat")
+
+NUM_BINS = 2000
+NUM_COUNTERS = 32
+NUM_HISTS = 8
+COUNTER_NAMES = {0: "trajectories", 1: "free", 2: "reflected", 3: "captured", 4: "completed_outward_escapes",
+                 5: "complete_evaporation", 6: "censored_captured", 7: "invalid_survival", 8: "initial_shift_failures",
+                 9: "final_reflection_shift_failures", 10: "numerical_failures", 11: "computational_truncations",
+                 12: "total_scatterings", 13: "rk_steps", 14: "events_dropped", 15: "rk_attempts"}
+REASON_BASE = 16
+HIST_NAMES = ["captured_dt", "captured_v2dt", "not_captured_dt", "not_captured_v2dt", "captured_dt_sq",
+              "captured_v2dt_sq", "not_captured_dt_sq", "not_captured_v2dt_sq"]
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "I/O error", -4: "no solar model", -5: "no such point",
+          -6: "capacity", -7: "iteration budget exhausted", -8: "cancelled", -9: "bad state"}
+
+
+class TrajRecord(ctypes.Structure):
+    _fields_ = [("trajectory_id", ctypes.c_uint64), ("number_of_scatterings", ctypes.c_uint64),
+                ("number_of_draws", ctypes.c_uint64), ("point", ctypes.c_uint32),
+                ("termination_reason", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("initial_time", ctypes.c_double), ("initial_position", ctypes.c_double * 3),
+                ("initial_velocity", ctypes.c_double * 3), ("final_time", ctypes.c_double),
+                ("final_position", ctypes.c_double * 3), ("final_velocity", ctypes.c_double * 3),
+                ("t_capture", ctypes.c_double), ("t_last_bound", ctypes.c_double),
+                ("t_final_unbinding_scatter", ctypes.c_double), ("t_boundary_escape", ctypes.c_double),
+                ("t_termination", ctypes.c_double), ("max_free_energy_drift_eV", ctypes.c_double),
+                ("max_free_energy_drift_rel", ctypes.c_double), ("lifetime_unbinding", ctypes.c_double)]
+
+
+class PointParams(ctypes.Structure):
+    _fields_ = [("mass_gev", ctypes.c_double), ("sigma_p_cm2", ctypes.c_double), ("sigma_e_cm2", ctypes.c_double),
+                ("fn_over_fp", ctypes.c_double), ("halo_v0_kms", ctypes.c_double), ("halo_vesc_kms", ctypes.c_double),
+                ("halo_vobs_kms", ctypes.c_double * 3), ("interpolation_points", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+class RunOpts(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint32), ("capture_mode", ctypes.c_int32), ("max_scatterings", ctypes.c_uint64),
+                ("max_free_steps", ctypes.c_uint64), ("boundary_radius_rsun", ctypes.c_double),
+                ("precision", ctypes.c_int32), ("threads_per_block", ctypes.c_uint32),
+                ("blocks_per_sm", ctypes.c_uint32), ("queue_chunk", ctypes.c_uint32),
+                ("iteration_budget", ctypes.c_uint64), ("time_limit_s", ctypes.c_double)]
+
+
+class WorkRange(ctypes.Structure):
+    _fields_ = [("point_id", ctypes.c_int32), ("reserved", ctypes.c_uint32), ("first_trajectory", ctypes.c_uint64),
+                ("count", ctypes.c_uint64)]
+
+
+class EvaporationEvent(ctypes.Structure):
+    _fields_ = [("trajectory_id", ctypes.c_uint64), ("lifetime_unbinding", ctypes.c_double)]
+
+
+class PointResults(ctypes.Structure):
+    _fields_ = [("counters", ctypes.c_uint64 * NUM_COUNTERS), ("histograms", ctypes.POINTER(ctypes.c_double)),
+                ("events", ctypes.POINTER(EvaporationEvent)), ("events_capacity", ctypes.c_uint64),
+                ("events_count", ctypes.c_uint64)]
+
+
+def point_params(mass_gev, sigma_p_cm2, sigma_e_cm2=1e-80, interpolation_points=1000, v0=220.0, vesc=544.0,
+                 vobs=(11.1, 232.2, 7.3), fn_over_fp=1.0):
+    """An SI contact point in low-mass mode with the Standard Halo Model of the reference configs."""
+    return PointParams(mass_gev, sigma_p_cm2, sigma_e_cm2, fn_over_fp, v0, vesc, (ctypes.c_double * 3)(*vobs),
+                       interpolation_points, 0)
+
+
+_lib = None
+
+
+def library():
+    """Loads libdms_cuda.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBRARY):
+        raise RuntimeError("libdms_cuda.so not built: run `make -C %s`" % HERE)
+    lib = ctypes.CDLL(LIBRARY)
+    c = ctypes
+    vp = c.c_void_p
+    lib.dms_create.argtypes = [c.POINTER(vp), c.c_int]
+    lib.dms_destroy.argtypes = [vp]
+    lib.dms_last_error.argtypes = [vp]
+    lib.dms_last_error.restype = c.c_char_p
+    lib.dms_cancel.argtypes = [vp]
+    lib.dms_load_solar_model.argtypes = [vp, c.c_char_p]
+    lib.dms_solar_table.argtypes = [vp, c.c_int, vp, c.c_size_t]
+    lib.dms_add_point.argtypes = [vp, c.POINTER(PointParams), c.POINTER(c.c_int)]
+    lib.dms_num_points.argtypes = [vp]
+    lib.dms_set_rate_grid.argtypes = [vp, c.c_int, vp, c.c_uint32]
+    lib.dms_get_rate_grid.argtypes = [vp, c.c_int, vp, c.c_uint32]
+    lib.dms_rate.argtypes = [vp, c.c_int, c.c_int, vp, vp, vp, c.c_size_t]
+    lib.dms_default_run_opts.argtypes = [c.POINTER(RunOpts)]
+    lib.dms_default_run_opts.restype = None
+    lib.dms_run.argtypes = [vp, c.POINTER(RunOpts), c.POINTER(WorkRange), c.c_int]
+    lib.dms_run_records.argtypes = [vp, c.POINTER(RunOpts), c.c_int, c.c_uint64, c.c_uint64, c.POINTER(TrajRecord), vp, vp]
+    lib.dms_get_results.argtypes = [vp, c.c_int, c.POINTER(PointResults)]
+    lib.dms_reset_results.argtypes = [vp, c.c_int]
+    lib.dms_num_bins.restype = c.c_int
+    lib.dms_last_kernel_ms.argtypes = [vp, c.POINTER(c.c_double)]
+    lib.dms_measure_fp64_peak.argtypes = [vp, c.POINTER(c.c_double)]
+    _lib = lib
+    return lib
+
+
+def run_opts(seed=1, capture_mode=False, max_scatterings=10 ** 14, max_free_steps=10 ** 12, boundary_rsun=2.0,
+             threads_per_block=0, blocks_per_sm=0, time_limit_s=0.0, iteration_budget=0):
+    o = RunOpts()
+    library().dms_default_run_opts(ctypes.byref(o))
+    o.seed = seed
+    o.capture_mode = int(bool(capture_mode))
+    o.max_scatterings = max_scatterings
+    o.max_free_steps = max_free_steps
+    o.boundary_radius_rsun = boundary_rsun
+    o.threads_per_block = threads_per_block
+    o.blocks_per_sm = blocks_per_sm
+    o.time_limit_s = time_limit_s
+    o.iteration_budget = iteration_budget
+    return o
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+class Engine:
+    """One engine context on one CUDA device."""
+
+    def __init__(self, device=0, solar_model=SOLAR_MODEL):
+        self.lib = library()
+        self.h = ctypes.c_void_p()
+        rc = self.lib.dms_create(ctypes.byref(self.h), device)
+        if rc != 0:
+            raise EngineError("dms_create failed (%s): no usable CUDA device %d" % (ERRORS.get(rc, rc), device))
+        if solar_model is not None:
+            self._check(self.lib.dms_load_solar_model(self.h, solar_model.encode()))
+
+    def _check(self, rc):
+        if rc < 0:
+            raise EngineError("%s: %s" % (ERRORS.get(rc, rc), self.lib.dms_last_error(self.h).decode()))
+        return rc
+
+    def close(self):
+        if self.h:
+            self.lib.dms_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solar_table(self, which):
+        n = self._check(self.lib.dms_solar_table(self.h, which, None, 0))
+        out = np.zeros(n)
+        self._check(self.lib.dms_solar_table(self.h, which, out.ctypes.data, n))
+        return out
+
+    def add_point(self, params):
+        pid = ctypes.c_int(-1)
+        self._check(self.lib.dms_add_point(self.h, ctypes.byref(params), ctypes.byref(pid)))
+        return pid.value
+
+    def set_rate_grid(self, point, grid):
+        g = np.ascontiguousarray(grid, dtype=np.float64)
+        self._check(self.lib.dms_set_rate_grid(self.h, point, g.ctypes.data, g.shape[0]))
+
+    def rate_grid(self, point, n):
+        g = np.zeros((n, n))
+        self._check(self.lib.dms_get_rate_grid(self.h, point, g.ctypes.data, n))
+        return g
+
+    def rate(self, point, r_km, v_kms, interpolated=True):
+        r = np.ascontiguousarray(r_km, dtype=np.float64)
+        v = np.ascontiguousarray(v_kms, dtype=np.float64)
+        out = np.zeros_like(r)
+        self._check(self.lib.dms_rate(self.h, point, int(interpolated), r.ctypes.data, v.ctypes.data, out.ctypes.data, r.size))
+        return out
+
+    def run(self, ranges, opts):
+        """ranges: iterable of (point_id, first_trajectory, count)."""
+        ranges = list(ranges)
+        arr = (WorkRange * len(ranges))(*[WorkRange(p, 0, f, c) for p, f, c in ranges])
+        self._check(self.lib.dms_run(self.h, ctypes.byref(opts), arr, len(ranges)))
+
+    def run_records(self, point, first, count, opts, histograms=False):
+        recs = (TrajRecord * count)()
+        hd = np.zeros((count, NUM_BINS)) if histograms else None
+        hv = np.zeros((count, NUM_BINS)) if histograms else None
+        self._check(self.lib.dms_run_records(self.h, ctypes.byref(opts), point, first, count, recs,
+                                             hd.ctypes.data if hd is not None else None,
+                                             hv.ctypes.data if hv is not None else None))
+        out = {"records": recs}
+        if histograms:
+            out["hist_dt"], out["hist_v2dt"] = hd, hv
+        return out
+
+    def results(self, point, events_capacity=1 << 20):
+        res = PointResults()
+        hist = np.zeros(NUM_HISTS * NUM_BINS)
+        events = (EvaporationEvent * events_capacity)()
+        res.histograms = hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        res.events = events
+        res.events_capacity = events_capacity
+        self._check(self.lib.dms_get_results(self.h, point, ctypes.byref(res)))
+        counters = {name: int(res.counters[k]) for k, name in COUNTER_NAMES.items()}
+        counters["reasons"] = [int(res.counters[REASON_BASE + k]) for k in range(11)]
+        n = min(res.events_count, events_capacity)
+        ev = np.array([(events[i].trajectory_id, events[i].lifetime_unbinding) for i in range(n)],
+                      dtype=[("trajectory_id", np.uint64), ("lifetime_unbinding", np.float64)])
+        return {"counters": counters, "histograms": hist.reshape(NUM_HISTS, NUM_BINS), "events": ev}
+
+    def last_kernel_ms(self):
+        ms = ctypes.c_double(0.0)
+        self._check(self.lib.dms_last_kernel_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def fp64_peak_tflops(self):
+        t = ctypes.c_double(0.0)
+        self._check(self.lib.dms_measure_fp64_peak(self.h, ctypes.byref(t)))
+        return t.value
+
+    def reset_results(self, point):
+        self._check(self.lib.dms_reset_results(self.h, point))

@@ -113,6 +113,12 @@ int dms_cancel(dms_ctx* ctx);
  * device: G*M(r), T(r), v_esc^2(r), n_e(r) and n_i(r) for the 63 isotope targets. */
 int dms_load_solar_model(dms_ctx* ctx, const char* path);
 
+/* Copies one radial table back from the device (Solar_Model's interpolation tables,
+ * include/Solar_Model.hpp:294-305): which = 0 knots r [km], 1 G*M [km^3/s^2], 2 T [GeV],
+ * 3 v_esc^2 [km^2/s^2], 4 n_e [1/km^3], 5 n_i [1/km^3] node-major (knots x 63).
+ * Returns the number of values (also when out is NULL) or a negative DMS_ERR_*. */
+int dms_solar_table(dms_ctx* ctx, int which, double* out, size_t capacity);
+
 /* ---- parameter points -------------------------------------------------------------------- */
 typedef struct
 {
@@ -131,6 +137,12 @@ typedef struct
  * Total_DM_Scattering_Rate_Computed at every node, src/Solar_Model.cpp:395-465). */
 int dms_add_point(dms_ctx* ctx, const dms_point_params* params, int* point_id);
 int dms_num_points(const dms_ctx* ctx);
+
+/* Replaces / reads the N x N total-rate grid of a point (N*N doubles, radius-major, 1/s):
+ * the rate_grid member of Solar_Model after Interpolate_Total_DM_Scattering_Rate
+ * (include/Solar_Model.hpp:309), for callers that build or cache the grid elsewhere. */
+int dms_set_rate_grid(dms_ctx* ctx, int point_id, const double* grid, uint32_t n);
+int dms_get_rate_grid(dms_ctx* ctx, int point_id, double* grid, uint32_t n);
 
 /* Scattering rate [1/s] of point `point_id` at radius r_km and speed v_kms, through the
  * interpolated grid (interpolated = 1) or the direct sum over targets (interpolated = 0).
@@ -152,6 +164,9 @@ typedef struct
 	uint32_t blocks_per_sm;            /* 0 = default */
 	uint32_t queue_chunk;              /* trajectories claimed per queue fetch; 0 = default */
 	uint64_t iteration_budget;         /* per-lane loop-iteration bound; 0 = default */
+	double time_limit_s;               /* wall-clock bound of one launch, enforced through the
+	                                      cancel flag; 0 = none (the reference's
+	                                      max_trajectory_wall_time_sec is per trajectory) */
 } dms_run_opts;
 
 typedef struct
@@ -194,6 +209,7 @@ int dms_run_records(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64
 #define DMS_CNT_TOTAL_SCATTERINGS         12
 #define DMS_CNT_RK_STEPS                  13   /* accepted free-propagation steps (work counter) */
 #define DMS_CNT_EVENTS_DROPPED            14   /* evaporation events beyond the buffer capacity */
+#define DMS_CNT_RK_ATTEMPTS               15   /* RK45 stage evaluations incl. rejected tries (work counter) */
 #define DMS_CNT_REASON_BASE               16   /* + DMS_REASON_*: trajectories per termination reason */
 #define DMS_NUM_COUNTERS                  32
 
@@ -229,6 +245,16 @@ int dms_reset_results(dms_ctx* ctx, int point_id);
 
 /* Sizes a caller needs to know. */
 int dms_num_bins(void);
+
+/* Device time [ms] of the last trajectory launch of dms_run / dms_run_records, measured with
+ * CUDA events on the context's stream around the kernel (no reference counterpart: the
+ * reference reports wall-clock computing_time only, src/Data_Generation.cpp:953-954). */
+int dms_last_kernel_ms(const dms_ctx* ctx, double* ms);
+
+/* Measures the device's FP64 FMA throughput [TFLOP/s, 2 FLOP per FMA] with a kernel of
+ * independent DFMA chains over every SM: the roofline denominator of the FP64 trajectory
+ * kernel (a diagnostic with no reference counterpart). */
+int dms_measure_fp64_peak(dms_ctx* ctx, double* tflops);
 
 #ifdef __cplusplus
 }
