@@ -26,6 +26,12 @@
 #include "../include/dms_philox.h"
 
 #define PI 3.14159265358979323846
+
+/* Work-unit marks for the op-counting build (oracle/opcount.hpp); no-ops otherwise. */
+#ifndef DMS_OPS_MARK
+#define DMS_OPS_MARK(kind)
+#define DMS_OPS_PHASE(kind)
+#endif
 #define SQRT_PI sqrt(PI) /* as the reference: sqrt(M_PI), not the rounded literal */
 #define PI_1_5 5.5683279968317078453
 
@@ -170,7 +176,7 @@ static int load_solar(dms_oracle* o, const char* path)
 		if(!fgets(line, sizeof line, f))
 			break;
 	size_t cap = 2048, rows = 0;
-	double* raw = malloc(cap * DMS_SOLAR_COLUMNS * sizeof(double));
+	double* raw = (double*)malloc(cap * DMS_SOLAR_COLUMNS * sizeof(double));
 	while(fgets(line, sizeof line, f))
 	{
 		double vals[DMS_SOLAR_COLUMNS];
@@ -197,7 +203,7 @@ static int load_solar(dms_oracle* o, const char* path)
 		if(rows + 2 >= cap)
 		{
 			cap *= 2;
-			raw = realloc(raw, cap * DMS_SOLAR_COLUMNS * sizeof(double));
+			raw = (double*)realloc(raw, cap * DMS_SOLAR_COLUMNS * sizeof(double));
 		}
 		memcpy(raw + (rows + 1) * DMS_SOLAR_COLUMNS, vals, sizeof vals);
 		rows++;
@@ -226,7 +232,7 @@ static int load_solar(dms_oracle* o, const char* path)
 	last[3] = DMS_PHOTOSPHERE_RHO_GCM3;
 
 	o->n = n;
-	o->r = malloc(n * sizeof(double));
+	o->r = (double*)malloc(n * sizeof(double));
 	for(int i = 0; i < n; i++) o->r[i] = raw[i * DMS_SOLAR_COLUMNS + 1] * DMS_RSUN_KM;
 
 	table1d* tabs[4] = {&o->gm, &o->temp, &o->vesc2, &o->n_e};
@@ -234,8 +240,8 @@ static int load_solar(dms_oracle* o, const char* path)
 	{
 		tabs[k]->n = n;
 		tabs[k]->x = o->r;
-		tabs[k]->y = calloc(n, sizeof(double));
-		tabs[k]->s = calloc(n, sizeof(double));
+		tabs[k]->y = (double*)calloc(n, sizeof(double));
+		tabs[k]->s = (double*)calloc(n, sizeof(double));
 	}
 	/* mass -> gravitational parameter G*M(r) [km^3/s^2]; temperature in GeV (natural) */
 	for(int i = 0; i < n; i++)
@@ -288,8 +294,8 @@ static int load_solar(dms_oracle* o, const char* path)
 		table1d* tb = &o->targets[t];
 		tb->n = n;
 		tb->x = o->r;
-		tb->y = calloc(n, sizeof(double));
-		tb->s = calloc(n, sizeof(double));
+		tb->y = (double*)calloc(n, sizeof(double));
+		tb->s = (double*)calloc(n, sizeof(double));
 		for(int i = 0; i < n; i++)
 		{
 			const double rho = raw[i * DMS_SOLAR_COLUMNS + 3] * 1.0e12; /* g/cm^3 -> kg/km^3 */
@@ -815,6 +821,8 @@ static int rk45_step(const dms_oracle* o, propagator_t* p)
 	for(;;)
 	{
 		inner++;
+		DMS_OPS_MARK(0);
+		DMS_OPS_PHASE(0);
 		const double dt = p->time_step;
 		double kr[6], kv[6], kp[6], ri;
 		kr[0] = dt * p->v_radial;
@@ -1355,6 +1363,7 @@ static int commit_event(const dms_oracle* o, sim_t* s, const event_t* local, dou
 /* Propagate_Freely, src/Simulation_Trajectory.cpp:762-1119 */
 static int propagate_freely(dms_oracle* o, sim_t* s, event_t* current)
 {
+	DMS_OPS_PHASE(2);
 	if(outward_escaping(o, current, s->max_distance))
 		return DMS_REASON_OUTWARD_ESCAPE;
 	if(uncaptured_bound(o, s, current))
@@ -1374,6 +1383,7 @@ static int propagate_freely(dms_oracle* o, sim_t* s, event_t* current)
 	if(!s->capture_mode && s->prev_time >= 0.0)
 		s->prev_time = 0.0;
 
+	DMS_OPS_PHASE(1);
 	while(steps < s->max_free_steps && outcome == DMS_REASON_MAX_FREE_STEPS)
 	{
 		const event_t before = prop_event(&prop);
@@ -1412,6 +1422,7 @@ static int propagate_freely(dms_oracle* o, sim_t* s, event_t* current)
 		const propagator_t prop_before = prop;
 		const double t_before = prop.time;
 		const int ok = rk45_step(o, &prop);
+		DMS_OPS_PHASE(1);
 		const double actual_dt = prop.time - t_before;
 		const double r_after = prop_radius(&prop);
 		const double v_after = prop_speed(&prop);
@@ -1535,6 +1546,7 @@ static int propagate_freely(dms_oracle* o, sim_t* s, event_t* current)
 				{
 					steps++;
 					retries = 0;
+					DMS_OPS_MARK(1);
 					commit_event(o, s, &boundary_ev, origin);
 					*current = inbound;
 					current->time += origin;
@@ -1551,6 +1563,7 @@ static int propagate_freely(dms_oracle* o, sim_t* s, event_t* current)
 		}
 		steps++;
 		retries = 0;
+		DMS_OPS_MARK(1);
 		const int captured_now = commit_event(o, s, &accepted, origin);
 		*current = accepted;
 		current->time += origin;
@@ -1745,12 +1758,14 @@ static void simulate(dms_oracle* o, sim_t* s, const event_t* ic, dms_traj_record
 		const int pr = propagate_freely(o, s, &cur);
 		if(pr == DMS_REASON_SCATTER && ev_radius(&cur) < DMS_RSUN_KM)
 		{
+			DMS_OPS_PHASE(2);
 			if(!scatter(o, &cur))
 			{
 				reason = DMS_REASON_NUMERICAL_FAILURE;
 				break;
 			}
 			nscat++;
+			DMS_OPS_MARK(2);
 			const int cap = update_capture_state(o, s, ev_radius(&cur), ev_speed(&cur), cur.time, 1);
 			reset_anchor(s, &cur);
 			if(s->capture_mode && cap)
@@ -1765,6 +1780,7 @@ static void simulate(dms_oracle* o, sim_t* s, const event_t* ic, dms_traj_record
 			break;
 		}
 	}
+	DMS_OPS_PHASE(3);
 	if(reason == DMS_REASON_UNKNOWN && nscat >= s->max_scatterings)
 		reason = DMS_REASON_MAX_SCATTERINGS;
 	s->t_termination = cur.time;
@@ -1863,7 +1879,7 @@ static void simulate(dms_oracle* o, sim_t* s, const event_t* ic, dms_traj_record
  */
 dms_oracle* dms_oracle_create(const char* path)
 {
-	dms_oracle* o = calloc(1, sizeof(dms_oracle));
+	dms_oracle* o = (dms_oracle*)calloc(1, sizeof(dms_oracle));
 	if(!o)
 		return NULL;
 	if(load_solar(o, path) != 0)
@@ -1926,7 +1942,7 @@ int dms_oracle_set_point(dms_oracle* o, const dms_point_params* p)
 	/* rate grid, Interpolate_Total_DM_Scattering_Rate src/Solar_Model.cpp:395-465 */
 	const unsigned int N = p->interpolation_points;
 	free(o->grid);
-	o->grid = malloc((size_t)N * N * sizeof(double));
+	o->grid = (double*)malloc((size_t)N * N * sizeof(double));
 	if(!o->grid)
 		return DMS_ERR_CAPACITY;
 	o->grid_n = (int)N;
@@ -2013,8 +2029,8 @@ int dms_oracle_run_records(dms_oracle* o, uint32_t seed, uint32_t point, int cap
 	s.max_free_steps = 1000000000000ULL;  /* DEFAULT_MAXIMUM_FREE_TIME_STEPS */
 	s.max_scatterings = max_scatterings;
 	s.max_distance = boundary_rsun * DMS_RSUN_KM;
-	double* dt_buf = malloc(DMS_NUM_BINS * sizeof(double));
-	double* v2_buf = malloc(DMS_NUM_BINS * sizeof(double));
+	double* dt_buf = (double*)malloc(DMS_NUM_BINS * sizeof(double));
+	double* v2_buf = (double*)malloc(DMS_NUM_BINS * sizeof(double));
 	s.dt_hist = dt_buf;
 	s.v2dt_hist = v2_buf;
 	for(uint64_t k = 0; k < count; k++)
@@ -2030,6 +2046,8 @@ int dms_oracle_run_records(dms_oracle* o, uint32_t seed, uint32_t point, int cap
 		o->trace = (trace != NULL && k == 0) ? trace : NULL;
 		o->trace_capacity = trace_capacity;
 		o->trace_length = 0;
+		DMS_OPS_MARK(3);
+		DMS_OPS_PHASE(3);
 		event_t ic = initial_conditions(o);
 		const int shift_ok = hyperbolic_kepler_shift(&ic, s.max_distance);
 		rec->initial_time = ic.time;
