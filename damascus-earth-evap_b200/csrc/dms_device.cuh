@@ -49,6 +49,7 @@ struct DevPoint
 	double avg_speed, eta0;
 	double grid_inv_r, grid_inv_v, grid_vmax;
 	const double* grid;    // grid_n x grid_n, radius-major
+	const float* grid_f;   // FP32 image of grid (mixed-precision kernel)
 	int grid_n;
 	int pad;
 	double sigma_t[DMS_NUM_TARGETS];
@@ -571,15 +572,21 @@ __device__ __forceinline__ double next_step_size(double current, double e0, doub
 	return sanitized_step(factor * current);
 }
 
-// Runge_Kutta_45_Step(Solar_Model&), src/Simulation_Trajectory.cpp:1487-1602; returns the
-// number of attempts made (negative when the step was forced at the minimum step size)
-__device__ __forceinline__ int rk45_step(const DevSolar& S, Prop& p)
+// One pass of the while(!accepted) loop of Runge_Kutta_45_Step(Solar_Model&),
+// src/Simulation_Trajectory.cpp:1492-1600, as its own unit so that lanes of a warp retry in
+// lock-step.  `inner` is the pass number (1-based).  Returns RK_ACCEPTED, RK_RETRY (state
+// unchanged, smaller time_step) or RK_FORCED (the minimum-step / retry-cap forced accept, for
+// which the reference returns false).
+enum RkResult : int
 {
-	p.time_step = sanitized_step(p.time_step);
-	int inner = 0;
-	for(;;)
+	RK_ACCEPTED = 0,
+	RK_RETRY = 1,
+	RK_FORCED = 2,
+};
+
+__device__ __forceinline__ int rk45_attempt(const DevSolar& S, Prop& p, int inner)
+{
 	{
-		inner++;
 		const double dt = p.time_step;
 		const double J = p.J;
 		double kr0, kr1, kr2, kr3, kr4, kr5, kv0, kv1, kv2, kv3, kv4, kv5, kp0, kp2, kp3, kp4, kp5, ri;
@@ -621,7 +628,7 @@ __device__ __forceinline__ int rk45_step(const DevSolar& S, Prop& p)
 			p.v_radial = v4;
 			p.phi = p4;
 			p.time_step = new_step;
-			return inner;
+			return RK_ACCEPTED;
 		}
 		if(new_step < DMS_RK45_ABS_MIN_STEP_S || inner >= DMS_RK45_MAX_INNER_RETRIES)
 		{
@@ -634,9 +641,10 @@ __device__ __forceinline__ int rk45_step(const DevSolar& S, Prop& p)
 				p.phi = p4;
 			}
 			p.time_step = DMS_RK45_ABS_MIN_STEP_S;
-			return -inner;
+			return RK_FORCED;
 		}
 		p.time_step = new_step;
+		return RK_RETRY;
 	}
 }
 

@@ -20,6 +20,10 @@ enum : unsigned int
 struct RunParams
 {
 	DevSolar S;
+	// FP32 images of the knot, G*M and G*M-slope tables (mixed-precision kernel only)
+	const float* sf_r;
+	const float* sf_gm;
+	const float* sf_gm_s;
 	const DevPoint* points;
 	int n_points;
 	// work: ranges and their prefix offsets (n_ranges + 1)
@@ -57,6 +61,10 @@ void Launch_Trajectories(const RunParams& p, int blocks, int threads, cudaStream
 void Launch_Rate_Grid(const DevSolar& S, const DevPoint* point, double* grid, int n, cudaStream_t stream);
 void Launch_Rate_Query(const DevSolar& S, const DevPoint* point, int interpolated, const double* r, const double* v, double* out,
                        size_t n, cudaStream_t stream);
+// mixed-precision (batched FP32) trajectory kernel and the FP32 image of a rate grid
+void Launch_Trajectories_Mixed(const RunParams& p, int blocks, int threads, cudaStream_t stream);
+void Launch_To_Float(const double* in, float* out, size_t n, cudaStream_t stream);
+int Trajectory_Mixed_Max_Blocks_Per_SM(int threads);
 int Trajectory_Kernel_Registers();
 int Trajectory_Max_Blocks_Per_SM(int threads);
 double Measure_FP64_Peak(int sm_count, cudaStream_t stream);

@@ -1,0 +1,514 @@
+// Lane state machine shared by the FP64 and the mixed-precision trajectory kernels: lane state,
+// work claims, trajectory start, free-segment start, capture bookkeeping, termination and
+// aggregation.  The free step itself (the Propagate_Freely loop body) is supplied by each form.
+#pragma once
+
+#include "dms_kernels.cuh"
+
+namespace dms
+{
+namespace lane
+{
+
+enum Phase : int
+{
+	PH_FETCH = 0,
+	PH_SEGMENT = 1,
+	PH_STEP = 2,
+	PH_FINAL = 3,
+	PH_DONE = 4,
+};
+
+
+// Trajectory state of a lane (TrajectoryBincount + Trajectory_Simulator members,
+// include/Simulation_Trajectory.hpp:53-154).
+template <class PropT, class EvT>
+struct LaneT
+{
+	uint64_t work;
+	int point;
+	Draws D;
+	Event cur;           // absolute event at segment boundaries and at termination
+	PropT pr;            // propagator of the current free segment (local time)
+	EvT before;          // Event_In_3D of the propagator at the start of the step (cached)
+	double origin;       // absolute time of the segment's local t = 0
+	double tau;          // remaining optical depth to the next scattering (minus_log_xi)
+	uint64_t seg_steps;
+	uint64_t nscat;
+	uint64_t steps;      // accepted free steps of the whole trajectory (work counter)
+	uint64_t attempts;   // RK45 attempts of the whole trajectory (work counter)
+	unsigned int retries;
+	int before_valid;
+	int in_rk;           // an RK45 step is in progress (retry pending)
+	int rk_inner;        // passes of the current RK45 step
+	double rate_before;  // scattering rate at the start of the step
+	double b_time, b_radius, b_phi, b_vr, b_step;  // propagator fields at the start of the step
+	int shift_ok;
+	int reason;
+	// capture / evaporation state
+	int is_captured;
+	int bound_state;
+	double t_capture, t_last_bound, t_final_unbinding;
+	double free_flight_E;
+	double max_drift_eV, max_drift_rel;
+	// bincount anchor (left-endpoint rule)
+	double prev_time, prev_r, prev_v2;
+	int bmin, bmax;
+};
+template <class Lane>
+__device__ __forceinline__ void accumulate_bincount(Lane& L, double2* hist, double r, double v2, double dt)
+{
+	// Accumulate_Bincount_Step, src/Simulation_Trajectory.cpp:640-669
+	if(!isfinite(dt) || dt <= 0.0)
+		return;
+	int bin = -1;
+	if(isfinite(r) && r >= 0.0 && r < DMS_BIN_MAX_KM)
+	{
+		bin = static_cast<int>(r / DMS_BIN_WIDTH_KM);
+		if(bin < 0) bin = 0;
+		if(bin >= DMS_NUM_BINS) bin = -1;
+	}
+	if(bin >= 0)
+	{
+		double2 h = hist[bin];
+		h.x += dt;
+		h.y += v2 * dt;
+		hist[bin] = h;
+		L.bmin = bin < L.bmin ? bin : L.bmin;
+		L.bmax = bin > L.bmax ? bin : L.bmax;
+	}
+}
+
+// Update_Capture_State, src/Simulation_Trajectory.cpp:689-760
+template <class Lane>
+__device__ __forceinline__ bool update_capture_state(const DevSolar& S, double m_dm, int capture_mode, Lane& L, double r, double v, double t, bool allow_new)
+{
+	if(capture_mode && !allow_new && !L.is_captured)
+		return false;
+	const double E = capture_energy_eV(S, m_dm, r, v);
+	const bool negative = E < 0.0;
+	if(!allow_new)
+	{
+		if(L.is_captured && isfinite(L.free_flight_E))
+		{
+			const double drift = fabs(E - L.free_flight_E);
+			if(isfinite(drift) && drift > L.max_drift_eV)
+				L.max_drift_eV = drift;
+			const double ref = fabs(L.free_flight_E);
+			const double scale = ref > DMS_FREE_ENERGY_DRIFT_REL_E_SCALE_EV ? ref : DMS_FREE_ENERGY_DRIFT_REL_E_SCALE_EV;
+			const double rel = drift / scale;
+			if(isfinite(rel) && rel > L.max_drift_rel)
+				L.max_drift_rel = rel;
+		}
+		if(L.bound_state && L.is_captured)
+			L.t_last_bound = t;
+		return false;
+	}
+	const int was_bound = L.bound_state;
+	L.bound_state = negative;
+	L.free_flight_E = E;
+	if(negative)
+	{
+		if(!L.is_captured)
+		{
+			L.is_captured = 1;
+			L.t_capture = t;
+			L.t_last_bound = t;
+		}
+		else if(!was_bound)
+			L.t_final_unbinding = NAN;
+		L.t_last_bound = t;
+		return true;
+	}
+	if(was_bound && L.is_captured)
+		L.t_final_unbinding = t;
+	return false;
+}
+
+template <class Lane>
+__device__ __forceinline__ bool uncaptured_bound(const DevSolar& S, double m_dm, const Lane& L, const Event& e)
+{
+	if(L.is_captured)
+		return false;
+	const double E = capture_energy_eV(S, m_dm, ev_radius(e), ev_speed(e));
+	if(isfinite(E) && E >= 0.0)
+		return false;
+	return true;
+}
+
+template <class Lane>
+__device__ __forceinline__ void set_final(Lane& L, const Event& local_or_abs, bool is_local, int reason)
+{
+	L.cur = local_or_abs;
+	if(is_local)
+		L.cur.t += L.origin;
+	L.reason = reason;
+}
+
+__device__ __forceinline__ void init_propagator(Prop& p, const Event& e) { prop_init(p, e); }
+
+// Start of a free segment: Simulate loop head + Propagate_Freely prologue,
+// src/Simulation_Trajectory.cpp:1311-1313, 762-805
+template <class Lane>
+__device__ __forceinline__ int segment_start(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, Lane& L)
+{
+	if(!(L.nscat < R.max_scatterings))
+	{
+		L.reason = DMS_REASON_MAX_SCATTERINGS;
+		return PH_FINAL;
+	}
+	if(outward_escaping(R.S, L.cur, R.boundary))
+	{
+		L.reason = DMS_REASON_OUTWARD_ESCAPE;
+		return PH_FINAL;
+	}
+	if(uncaptured_bound(R.S, m_dm, L, L.cur))
+	{
+		L.reason = DMS_REASON_NUMERICAL_FAILURE;
+		return PH_FINAL;
+	}
+	L.origin = L.cur.t;
+	Event local = L.cur;
+	local.t = 0.0;
+	init_propagator(L.pr, local);
+	L.tau = -dms_log(L.D.positive_unit());
+	L.seg_steps = 0;
+	L.retries = 0;
+	L.before_valid = 0;
+	L.in_rk = 0;
+	if(!R.capture_mode && L.prev_time >= 0.0)
+		L.prev_time = 0.0;
+	return PH_STEP;
+}
+
+__device__ __forceinline__ bool is_numerical_termination(int r)
+{
+	return r == DMS_REASON_NUMERICAL_FAILURE || r == DMS_REASON_NON_FINITE_STATE || r == DMS_REASON_SPEED_LIMIT ||
+	       r == DMS_REASON_ENERGY_DRIFT_ESCAPE || r == DMS_REASON_UNKNOWN;
+}
+
+__device__ __forceinline__ bool is_computational_truncation(int r)
+{
+	return r == DMS_REASON_WALL_TIME_LIMIT || r == DMS_REASON_MAX_FREE_STEPS || r == DMS_REASON_MAX_SCATTERINGS;
+}
+
+// Termination: tail of Simulate (src/Simulation_Trajectory.cpp:1349-1399), classification and
+// aggregation of simulate_one_trajectory (src/Data_Generation.cpp:745-861).
+template <class Lane>
+__device__ __noinline__ void finalize(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, Lane& L, double2* hist)
+{
+	const DevSolar& S = R.S;
+	int reason = L.reason;
+	int survival_valid = 1, event_observed = 0, boundary_escape = 0, invalid_escape = 0;
+	double t_boundary = NAN;
+	const double t_term = L.cur.t;
+	uint32_t flags = 0;
+	if(L.shift_ok)
+	{
+		flags |= DMS_REC_SHIFT_OK;
+		if(L.is_captured)
+		{
+			const double r_f = ev_radius(L.cur), v_f = ev_speed(L.cur);
+			const double vesc_f = solar_vesc(S, r_f);
+			const double E_f = 0.5 * m_dm * ((v_f * v_f - vesc_f * vesc_f) / (DMS_C_KMS * DMS_C_KMS)) / 1.0e-9;
+			if(reason == DMS_REASON_OUTWARD_ESCAPE && E_f >= 0.0)
+			{
+				if(isfinite(L.t_final_unbinding))
+				{
+					boundary_escape = 1;
+					t_boundary = t_term;
+					event_observed = 1;
+				}
+				else
+				{
+					reason = DMS_REASON_ENERGY_DRIFT_ESCAPE;
+					survival_valid = 0;
+					invalid_escape = 1;
+				}
+			}
+		}
+		switch(reason)
+		{
+			case DMS_REASON_ENERGY_DRIFT_ESCAPE:
+			case DMS_REASON_NUMERICAL_FAILURE:
+			case DMS_REASON_NON_FINITE_STATE:
+			case DMS_REASON_SPEED_LIMIT:
+			case DMS_REASON_WALL_TIME_LIMIT:
+			case DMS_REASON_MAX_FREE_STEPS:
+			case DMS_REASON_MAX_SCATTERINGS:
+			case DMS_REASON_UNKNOWN: survival_valid = 0; break;
+			default: break;
+		}
+		if(L.is_captured && !event_observed)
+		{
+			L.t_final_unbinding = NAN;
+			if(reason != DMS_REASON_CAPTURE_MODE)
+				survival_valid = 0;
+		}
+		if(L.is_captured) flags |= DMS_REC_CAPTURED;
+		if(event_observed) flags |= DMS_REC_EVENT_OBSERVED;
+		if(survival_valid) flags |= DMS_REC_SURVIVAL_VALID;
+		if(boundary_escape) flags |= DMS_REC_BOUNDARY_ESCAPE;
+		if(invalid_escape) flags |= DMS_REC_INVALID_ESCAPE;
+		if(!L.is_captured && reason == DMS_REASON_OUTWARD_ESCAPE)
+		{
+			if(L.nscat == 0)
+				flags |= DMS_REC_FREE;
+			else
+			{
+				const double rf = ev_radius(L.cur);
+				const double vesc = sqrt(2 * DMS_GMSUN_KM3S2 / rf);
+				if(rf > DMS_RSUN_KM && ev_speed(L.cur) > vesc)
+				{
+					flags |= DMS_REC_REFLECTED;
+					Event fin = L.cur;
+					if(hyperbolic_kepler_shift(fin, DMS_AU_KM))
+						flags |= DMS_REC_REFLECT_SHIFT_OK;
+				}
+			}
+		}
+	}
+	else
+	{
+		reason = DMS_REASON_NUMERICAL_FAILURE;
+		survival_valid = 0;
+	}
+	const bool invalid = invalid_escape || reason == DMS_REASON_ENERGY_DRIFT_ESCAPE;
+	const bool valid = survival_valid && !invalid;
+	const bool observed = valid && event_observed;
+	const double life = observed ? L.t_final_unbinding - L.t_capture : -1.0;
+	const double lifetime = (L.is_captured && isfinite(life) && life >= 0.0) ? life : -1.0;
+
+	const int b0 = L.bmin, b1 = L.bmax;
+	if(R.records != nullptr)
+	{
+		dms_traj_record& rec = R.records[L.work - 0];
+		rec.number_of_scatterings = L.nscat;
+		rec.number_of_draws = L.D.index;
+		rec.termination_reason = static_cast<uint32_t>(reason);
+		rec.flags = flags;
+		rec.final_time = L.cur.t;
+		rec.final_position[0] = L.cur.x.x;
+		rec.final_position[1] = L.cur.x.y;
+		rec.final_position[2] = L.cur.x.z;
+		rec.final_velocity[0] = L.cur.v.x;
+		rec.final_velocity[1] = L.cur.v.y;
+		rec.final_velocity[2] = L.cur.v.z;
+		rec.t_capture = L.shift_ok ? L.t_capture : -1.0;
+		rec.t_last_bound = L.shift_ok ? L.t_last_bound : -1.0;
+		rec.t_final_unbinding_scatter = L.shift_ok ? L.t_final_unbinding : NAN;
+		rec.t_boundary_escape = t_boundary;
+		rec.t_termination = L.shift_ok ? t_term : -1.0;
+		rec.max_free_energy_drift_eV = L.max_drift_eV;
+		rec.max_free_energy_drift_rel = L.max_drift_rel;
+		rec.lifetime_unbinding = lifetime;
+		if(R.rec_hist_dt != nullptr)
+		{
+			double* hd = R.rec_hist_dt + L.work * DMS_NUM_BINS;
+			double* hv = R.rec_hist_v2dt + L.work * DMS_NUM_BINS;
+			for(int b = b0; b <= b1; b++)
+			{
+				const double2 h = hist[b];
+				hd[b] = h.x;
+				hv[b] = h.y;
+			}
+		}
+	}
+	else
+	{
+		unsigned long long* c = R.counters + static_cast<size_t>(L.point) * DMS_NUM_COUNTERS;
+		atomicAdd(c + DMS_CNT_TRAJECTORIES, 1ULL);
+		atomicAdd(c + DMS_CNT_TOTAL_SCATTERINGS, static_cast<unsigned long long>(L.nscat));
+		atomicAdd(c + DMS_CNT_RK_STEPS, static_cast<unsigned long long>(L.steps));
+		atomicAdd(c + DMS_CNT_RK_ATTEMPTS, static_cast<unsigned long long>(L.attempts));
+		atomicAdd(c + DMS_CNT_REASON_BASE + reason, 1ULL);
+		if(!L.shift_ok)
+		{
+			atomicAdd(c + DMS_CNT_INITIAL_SHIFT_FAILURES, 1ULL);
+			atomicAdd(c + DMS_CNT_NUMERICAL_FAILURES, 1ULL);
+		}
+		else if(is_numerical_termination(reason))
+			atomicAdd(c + DMS_CNT_NUMERICAL_FAILURES, 1ULL);
+		if(is_computational_truncation(reason))
+			atomicAdd(c + DMS_CNT_COMPUTATIONAL_TRUNCATIONS, 1ULL);
+		int hist_slot = -1;
+		if(L.is_captured)
+		{
+			atomicAdd(c + DMS_CNT_CAPTURED, 1ULL);
+			if(!R.capture_mode)
+			{
+				atomicAdd(c + (event_observed ? DMS_CNT_COMPLETE_EVAPORATION : DMS_CNT_INVALID_SURVIVAL), 1ULL);
+				hist_slot = 0;
+				if(lifetime >= 0.0)
+				{
+					const unsigned long long k = atomicAdd(R.event_count + L.point, 1ULL);
+					if(k < R.event_capacity)
+					{
+						dms_evaporation_event ev;
+						ev.trajectory_id = L.D.traj + 1;
+						ev.lifetime_unbinding = lifetime;
+						R.events[static_cast<size_t>(L.point) * R.event_capacity + k] = ev;
+					}
+					else
+						atomicAdd(c + DMS_CNT_EVENTS_DROPPED, 1ULL);
+				}
+			}
+		}
+		else if(reason == DMS_REASON_OUTWARD_ESCAPE)
+		{
+			atomicAdd(c + DMS_CNT_COMPLETED_OUTWARD, 1ULL);
+			if(!R.capture_mode)
+			{
+				hist_slot = 2;
+				if(flags & DMS_REC_FREE)
+					atomicAdd(c + DMS_CNT_FREE, 1ULL);
+				else if(flags & DMS_REC_REFLECTED)
+				{
+					atomicAdd(c + DMS_CNT_REFLECTED, 1ULL);
+					if(!(flags & DMS_REC_REFLECT_SHIFT_OK))
+					{
+						atomicAdd(c + DMS_CNT_FINAL_REFLECTION_SHIFT_FAILURES, 1ULL);
+						atomicAdd(c + DMS_CNT_NUMERICAL_FAILURES, 1ULL);
+					}
+				}
+			}
+		}
+		if(hist_slot >= 0)
+		{
+			double* h = R.hists + static_cast<size_t>(L.point) * DMS_NUM_HISTS * DMS_NUM_BINS;
+			double* h_dt = h + (hist_slot + 0) * DMS_NUM_BINS;
+			double* h_v2 = h + (hist_slot + 1) * DMS_NUM_BINS;
+			double* h_dt_sq = h + (hist_slot + 4) * DMS_NUM_BINS;
+			double* h_v2_sq = h + (hist_slot + 5) * DMS_NUM_BINS;
+			for(int b = b0; b <= b1; b++)
+			{
+				const double2 x = hist[b];
+				if(x.x != 0.0 || x.y != 0.0)
+				{
+					atomicAdd(h_dt + b, x.x);
+					atomicAdd(h_v2 + b, x.y);
+					atomicAdd(h_dt_sq + b, x.x * x.x);
+					atomicAdd(h_v2_sq + b, x.y * x.y);
+				}
+			}
+		}
+	}
+	for(int b = b0; b <= b1; b++) hist[b] = make_double2(0.0, 0.0);
+}
+
+// Picks up work index `w`: trajectory start = Initial_Conditions + Hyperbolic_Kepler_Shift and the
+// Simulate prologue (src/Data_Generation.cpp:747-761, src/Simulation_Trajectory.cpp:1284-1308).
+template <class Lane>
+__device__ __forceinline__ int start_trajectory(const RunParams& R, Lane& L, uint64_t w, const DevPoint*& P, double& m_dm)
+{
+	int k = 0;
+	while(k + 1 < R.n_ranges && w >= R.range_offset[k + 1]) k++;
+	L.work = w;
+	L.point = R.range_point[k];
+	P = R.points + L.point;
+	m_dm = __ldg(&P->m_dm);
+	L.D.seed = R.seed;
+	L.D.point = static_cast<uint32_t>(L.point);
+	L.D.traj = R.range_first[k] + (w - R.range_offset[k]);
+	L.D.index = 0;
+	L.nscat = 0;
+	L.steps = 0;
+	L.attempts = 0;
+	L.is_captured = 0;
+	L.bound_state = 0;
+	L.t_capture = -1.0;
+	L.t_last_bound = -1.0;
+	L.t_final_unbinding = NAN;
+	L.free_flight_E = NAN;
+	L.max_drift_eV = 0.0;
+	L.max_drift_rel = 0.0;
+	L.prev_time = -1.0;
+	L.prev_r = 0.0;
+	L.prev_v2 = 0.0;
+	L.bmin = DMS_NUM_BINS;
+	L.bmax = -1;
+	L.reason = DMS_REASON_UNKNOWN;
+	Event ic;
+	const bool ic_ok = initial_conditions(R.S, P, L.D, ic, R.ic_max_attempts);
+	if(!ic_ok)
+		atomicOr(R.status, STATUS_IC_REJECTION);
+	L.shift_ok = ic_ok && hyperbolic_kepler_shift(ic, R.boundary);
+	L.cur = ic;
+	if(R.records != nullptr)
+	{
+		dms_traj_record& rec = R.records[w];
+		rec.trajectory_id = L.D.traj;
+		rec.point = static_cast<uint32_t>(L.point);
+		rec.reserved = 0;
+		rec.initial_time = ic.t;
+		rec.initial_position[0] = ic.x.x;
+		rec.initial_position[1] = ic.x.y;
+		rec.initial_position[2] = ic.x.z;
+		rec.initial_velocity[0] = ic.v.x;
+		rec.initial_velocity[1] = ic.v.y;
+		rec.initial_velocity[2] = ic.v.z;
+	}
+	if(!L.shift_ok)
+	{
+		L.reason = DMS_REASON_NUMERICAL_FAILURE;
+		return PH_FINAL;
+	}
+	return PH_SEGMENT;
+}
+
+template <class Lane, class Step>
+__device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
+{
+	const int lane_id = blockIdx.x * blockDim.x + threadIdx.x;
+	double2* hist = R.lane_hist + static_cast<size_t>(lane_id) * DMS_NUM_BINS;
+	Lane L;
+	const DevPoint* P = R.points;
+	double m_dm = 0.0;
+	int phase = PH_FETCH;
+	const unsigned int lane_bit = 1u << (threadIdx.x & 31);
+	for(uint64_t iter = 0;; iter++)
+	{
+		if((iter & 1023) == 1023)
+		{
+			if(*R.cancel != 0)
+			{
+				atomicOr(R.status, STATUS_CANCELLED);
+				break;
+			}
+			if(iter > R.iteration_budget)
+			{
+				atomicOr(R.status, STATUS_BUDGET);
+				break;
+			}
+		}
+		if(phase == PH_FETCH)
+		{
+			// warp-aggregated claim of one work index per lane that needs one
+			const unsigned int mask = __activemask();
+			const int leader = __ffs(mask) - 1;
+			const unsigned int rank = __popc(mask & (lane_bit - 1u));
+			unsigned long long base = 0;
+			if((threadIdx.x & 31) == leader)
+				base = atomicAdd(R.queue_head, static_cast<unsigned long long>(__popc(mask)));
+			base = __shfl_sync(mask, base, leader);
+			const uint64_t w = base + rank;
+			if(w >= R.total)
+				break;
+			phase = start_trajectory(R, L, w, P, m_dm);
+		}
+		if(phase == PH_SEGMENT)
+			phase = segment_start(R, P, m_dm, L);
+		if(phase == PH_STEP)
+			phase = step(R, P, m_dm, L, hist);
+		if(phase == PH_FINAL)
+		{
+			finalize(R, P, m_dm, L, hist);
+			phase = PH_FETCH;
+		}
+	}
+	if(phase != PH_FETCH && L.bmax >= L.bmin)
+		for(int b = L.bmin; b <= L.bmax; b++) hist[b] = make_double2(0.0, 0.0);
+}
+
+}	// namespace lane
+}	// namespace dms
