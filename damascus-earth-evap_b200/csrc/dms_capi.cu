@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <thread>
@@ -687,6 +688,175 @@ int dms_reset_results(dms_ctx* ctx, int point_id)
 	DMS_CUDA(ctx, cudaMemset(ctx->d_counters + static_cast<size_t>(point_id) * DMS_NUM_COUNTERS, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_hists + static_cast<size_t>(point_id) * DMS_NUM_HISTS * DMS_NUM_BINS, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_event_count + point_id, 0, sizeof(unsigned long long)));
+	return DMS_OK;
+}
+
+}	// extern "C"
+
+// ---- dms_run_records_noalloc -----------------------------------------------------------------
+// Callers that cannot allocate device memory while they run trajectories: a host whose own
+// caching allocator reserved the device's memory up front, or a service that fixes its memory
+// budget before any work arrives and must not fail on an allocation later.  For them this
+// entry point writes into the caller's device buffers and keeps its scratch in the array
+// below, which is part of the library's device image: every device that loads the library
+// holds these 4 MiB until the process exits.
+//
+// Scratch layout (bytes): 0 work-queue head (u64), 8 status word (u32), 64 range start (u64),
+// 72 range offsets {0, count} (2 x u64), 96 range point (i32); from 256 one 2000-bin
+// (dt, v2dt) histogram row per lane, DMS_NOALLOC_MAX_TRAJECTORIES rows.
+static __device__ __align__(256) unsigned char dms_noalloc_scratch[DMS_NOALLOC_SCRATCH_BYTES];
+
+namespace
+{
+constexpr size_t NOALLOC_HEADER = 256;
+static_assert(DMS_NOALLOC_SCRATCH_BYTES == NOALLOC_HEADER + sizeof(double2) * DMS_NUM_BINS * DMS_NOALLOC_MAX_TRAJECTORIES,
+              "scratch size must match its layout");
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// Address of the scratch array on the context's device (current), looked up once per device.
+int Noalloc_Scratch(dms_ctx* ctx, unsigned char** out)
+{
+	if(ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "dms_run_records_noalloc: device index out of range");
+	std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+	if(g_noalloc_ptr[ctx->device] == nullptr)
+	{
+		unsigned char* ptr = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), dms_noalloc_scratch);
+		if(e != cudaSuccess || ptr == nullptr)
+			return Fail(ctx, DMS_ERR_CUDA, std::string("dms_run_records_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+		g_noalloc_ptr[ctx->device] = ptr;
+	}
+	*out = g_noalloc_ptr[ctx->device];
+	return DMS_OK;
+}
+
+// The array keeps whatever the previous call left, so this clears everything the trajectory
+// kernel expects to start at zero (queue head, status word, the lane rows in use) and the
+// caller's outputs (records, histogram rows), and writes the work range.
+__global__ void noalloc_prepare_kernel(unsigned char* scratch, uint64_t first, uint64_t count, int point, uint64_t lanes,
+                                       unsigned char* records, double* hist_dt, double* hist_v2dt)
+{
+	const uint64_t tid = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+	const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+	if(tid == 0)
+	{
+		*reinterpret_cast<unsigned long long*>(scratch + 0) = 0ULL;
+		*reinterpret_cast<unsigned int*>(scratch + 8) = 0u;
+		*reinterpret_cast<uint64_t*>(scratch + 64) = first;
+		reinterpret_cast<uint64_t*>(scratch + 72)[0] = 0;
+		reinterpret_cast<uint64_t*>(scratch + 72)[1] = count;
+		*reinterpret_cast<int32_t*>(scratch + 96) = point;
+	}
+	double2* rows = reinterpret_cast<double2*>(scratch + NOALLOC_HEADER);
+	for(uint64_t k = tid; k < lanes * DMS_NUM_BINS; k += stride) rows[k] = make_double2(0.0, 0.0);
+	for(uint64_t k = tid; k < count * sizeof(dms_traj_record); k += stride) records[k] = 0;
+	if(hist_dt != nullptr)
+		for(uint64_t k = tid; k < count * DMS_NUM_BINS; k += stride)
+		{
+			hist_dt[k] = 0.0;
+			hist_v2dt[k] = 0.0;
+		}
+}
+}	// namespace
+
+extern "C" {
+
+int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64_t first, uint64_t count,
+                            dms_traj_record* d_records, double* d_hist_dt, double* d_hist_v2dt)
+{
+	if(!ctx)
+		return DMS_ERR_INVALID_ARGUMENT;
+	int rc = Check_Run_Opts(ctx, opts);
+	if(rc != DMS_OK)
+		return rc;
+	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
+		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	if(count > DMS_NOALLOC_MAX_TRAJECTORIES)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT,
+		            "dms_run_records_noalloc: " + std::to_string(count) + " trajectories requested, at most " +
+		                std::to_string(DMS_NOALLOC_MAX_TRAJECTORIES) + " fit the fixed device scratch of one call");
+	if(count == 0)
+		return DMS_OK;
+	if(!d_records || ((d_hist_dt == nullptr) != (d_hist_v2dt == nullptr)))
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "records buffer required; histograms need both buffers");
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	unsigned char* scratch = nullptr;
+	rc = Noalloc_Scratch(ctx, &scratch);
+	if(rc != DMS_OK)
+		return rc;
+	const int threads = 32;
+	const int blocks = static_cast<int>((count + threads - 1) / threads);
+	const uint64_t lanes = static_cast<uint64_t>(blocks) * threads;
+
+	RunParams p{};
+	p.S = ctx->dsolar;
+	p.points = ctx->d_points;
+	p.n_points = static_cast<int>(ctx->points.size());
+	p.range_first = reinterpret_cast<const uint64_t*>(scratch + 64);
+	p.range_offset = reinterpret_cast<const uint64_t*>(scratch + 72);
+	p.range_point = reinterpret_cast<const int32_t*>(scratch + 96);
+	p.n_ranges = 1;
+	p.total = count;
+	p.queue_head = reinterpret_cast<unsigned long long*>(scratch + 0);
+	p.status = reinterpret_cast<unsigned int*>(scratch + 8);
+	p.lane_hist = reinterpret_cast<double2*>(scratch + NOALLOC_HEADER);
+	p.seed = opts->seed;
+	p.capture_mode = opts->capture_mode ? 1 : 0;
+	p.max_scatterings = opts->max_scatterings;
+	p.max_free_steps = opts->max_free_steps;
+	p.boundary = opts->boundary_radius_rsun * DMS_RSUN_KM;
+	p.iteration_budget = opts->iteration_budget ? opts->iteration_budget : ~0ULL;
+	p.ic_max_attempts = 1 << 20;
+	p.counters = ctx->d_counters;
+	p.hists = ctx->d_hists;
+	p.events = ctx->d_events;
+	p.event_count = ctx->d_event_count;
+	p.event_capacity = ctx->event_capacity;
+	p.records = d_records;
+	p.rec_hist_dt = d_hist_dt;
+	p.rec_hist_v2dt = d_hist_v2dt;
+	p.cancel = ctx->d_cancel;
+
+	*ctx->h_cancel = 0;
+	noalloc_prepare_kernel<<<8, 256, 0, ctx->stream>>>(scratch, first, count, point_id, lanes, reinterpret_cast<unsigned char*>(d_records),
+	                                                   d_hist_dt, d_hist_v2dt);
+	DMS_CUDA(ctx, cudaGetLastError());
+	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+	Launch_Trajectories(p, blocks, threads, ctx->stream);
+	DMS_CUDA(ctx, cudaGetLastError());
+	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+	const auto start = std::chrono::steady_clock::now();
+	bool cancelled_by_limit = false;
+	for(;;)
+	{
+		const cudaError_t q = cudaStreamQuery(ctx->stream);
+		if(q == cudaSuccess)
+			break;
+		if(q != cudaErrorNotReady)
+			return Fail(ctx, DMS_ERR_CUDA, std::string("trajectory kernel: ") + cudaGetErrorString(q));
+		if(opts->time_limit_s > 0.0 && !cancelled_by_limit &&
+		   std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count() > opts->time_limit_s)
+		{
+			*reinterpret_cast<volatile int*>(ctx->h_cancel) = 1;
+			cancelled_by_limit = true;
+		}
+		std::this_thread::sleep_for(std::chrono::microseconds(200));
+	}
+	float kernel_ms = 0.0f;
+	DMS_CUDA(ctx, cudaEventElapsedTime(&kernel_ms, ctx->ev_start, ctx->ev_stop));
+	ctx->last_kernel_ms = kernel_ms;
+	unsigned int status = 0;
+	DMS_CUDA(ctx, cudaMemcpy(&status, scratch + 8, sizeof status, cudaMemcpyDeviceToHost));
+	if(status & STATUS_CANCELLED)
+		return Fail(ctx, DMS_ERR_CANCELLED, cancelled_by_limit ? "run cancelled: wall-clock limit reached" : "run cancelled");
+	if(status & STATUS_BUDGET)
+		return Fail(ctx, DMS_ERR_BUDGET, "run stopped: per-lane iteration budget exhausted");
+	if(status & STATUS_IC_REJECTION)
+		ctx->error = "warning: an initial-condition rejection loop hit its attempt bound";
 	return DMS_OK;
 }
 
