@@ -38,12 +38,13 @@ SAMPLE_SIZE = 8192
 METRIC = "scatterings/s & trajectories/s on 1 B200, batched-FP32 vs plain-FP64 form"
 WORKLOAD = ("Parameter-point evaporation (config 1): SI contact m=0.3 GeV sigma_n=1e-36 cm2, AGSS09, SHM, "
             "1000x1000 rate grid, max 1e6 scatterings, seed 7; %d trajectories per GPU per step (>= 8192 captures)" % TRAJECTORIES)
-# Algorithmic FP64 operations (add/sub/mul/div/sqrt, one each; transcendental = 1) per unit of
-# work, counted from the source of the path: per RK45 attempt, per accepted free step (event
-# reconstruction, rate lookups, 4-piece optical depth, bincount, energy), per scattering
-# (63-target rate sum, target velocity rejection, kinematics) and per trajectory (initial
-# conditions and Kepler shift).
-FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ = 217.0, 390.0, 2100.0, 800.0
+# Algorithmic FP64 operations per unit of work (add, sub, mul, div, sqrt and each elementary
+# function count one), counted by the instrumented oracle build (oracle/liboracle_ops.so) on
+# this parameter point in Parameter-point (normal) mode: per RK45 attempt, per accepted free
+# step (event reconstruction, 4-piece optical depth, bincount, energy), per scattering
+# (64-channel rate sum, free-gas target velocity, kinematics) and per trajectory (initial
+# conditions, Kepler shift, classification).
+FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ = 214.8, 622.3, 2455.0, 3374.0
 
 
 def log(*a):
@@ -189,6 +190,18 @@ def run_reference_arm(args):
 
 # ------------------------------------------------------------------------------------------
 # engine arm
+def add_results(acc, res):
+    """Running sum of Engine.results() dictionaries (counters, histograms, events)."""
+    import numpy as np
+    if acc is None:
+        return {"counters": dict(res["counters"]), "histograms": res["histograms"].copy(), "events": res["events"].copy()}
+    for k, v in res["counters"].items():
+        acc["counters"][k] = [a + b for a, b in zip(acc["counters"][k], v)] if k == "reasons" else acc["counters"][k] + v
+    acc["histograms"] += res["histograms"]
+    acc["events"] = np.concatenate([acc["events"], res["events"]])
+    return acc
+
+
 def run_engine_arm(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -205,9 +218,13 @@ def run_engine_arm(args):
         dist.init_process_group("nccl", device_id=torch.device("cuda", local_rank),
                                 timeout=__import__("datetime").timedelta(seconds=600))
     import dms_b200
+    import dms_stats
     engine = dms_b200.Engine(local_rank)
     pid = engine.add_point(dms_b200.point_params(MASS_GEV, SIGMA_CM2, interpolation_points=GRID_N))
-    opts = dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT, time_limit_s=600.0)
+    opts = {prec: dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT, time_limit_s=600.0,
+                                    precision=prec)
+            for prec in (dms_b200.PRECISION_FP64, dms_b200.PRECISION_MIXED)}
+    fp64, mixed = dms_b200.PRECISION_FP64, dms_b200.PRECISION_MIXED
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     peak = engine.fp64_peak_tflops()
 
@@ -219,29 +236,35 @@ def run_engine_arm(args):
     def ids(step):
         return (step * world + rank) * TRAJECTORIES
 
-    # warm-up
+    def timed_steps(prec, first_step, events_capacity):
+        """K steps of one form: device time of the launches and the summed results."""
+        clocks = ClockSampler(local_rank)
+        clocks.start()
+        barrier()
+        ms = 0.0
+        acc = None
+        min_captured = None
+        for s in range(args.steps):
+            engine.reset_results(pid)
+            engine.run([(pid, ids(first_step + s), TRAJECTORIES)], opts[prec])
+            ms += engine.last_kernel_ms()
+            res = engine.results(pid, events_capacity=events_capacity)
+            acc = add_results(acc, res)
+            c = res["counters"]["captured"]
+            min_captured = c if min_captured is None else min(min_captured, c)
+            flush.zero_()
+        barrier()
+        return ms, acc, min_captured, clocks.stop()
+
+    # warm-up (both forms)
     for w in range(args.warmup):
-        engine.reset_results(pid)
-        engine.run([(pid, ids(w), TRAJECTORIES)], opts)
-        flush.zero_()
-    # timed region: device time of the trajectory launches
-    clocks = ClockSampler(local_rank)
-    clocks.start()
-    barrier()
-    dev_ms = 0.0
-    tot = {"trajectories": 0, "total_scatterings": 0, "captured": 0, "rk_steps": 0, "rk_attempts": 0}
-    min_captured = None
-    for s in range(args.steps):
-        engine.reset_results(pid)
-        engine.run([(pid, ids(args.warmup + s), TRAJECTORIES)], opts)
-        dev_ms += engine.last_kernel_ms()
-        c = engine.results(pid, events_capacity=1)["counters"]
-        for k in tot:
-            tot[k] += c[k]
-        min_captured = c["captured"] if min_captured is None else min(min_captured, c["captured"])
-        flush.zero_()
-    barrier()
-    clock_info = clocks.stop()
+        for prec in (fp64, mixed):
+            engine.reset_results(pid)
+            engine.run([(pid, ids(w), TRAJECTORIES)], opts[prec])
+            flush.zero_()
+    # timed region: FP64 form (the headline), then the mixed form on the same trajectory ids
+    dev_ms, tot, min_captured, clock_info = timed_steps(fp64, args.warmup, 1 << 16)
+    mix_ms, mix_tot, _, mix_clocks = timed_steps(mixed, args.warmup, 1 << 16) if not args.no_mixed else (0.0, None, 0, None)
     # e2e: through the C ABI with host buffers; every step copies its work range in and its
     # counters, histograms and evaporation events out
     barrier()
@@ -250,25 +273,30 @@ def run_engine_arm(args):
     d2h_bytes = 0
     for s in range(args.steps):
         engine.reset_results(pid)
-        engine.run([(pid, ids(args.warmup + args.steps + s), TRAJECTORIES)], opts)
+        engine.run([(pid, ids(args.warmup + args.steps + s), TRAJECTORIES)], opts[fp64])
         res = engine.results(pid, events_capacity=1 << 16)
         e2e_scat += res["counters"]["total_scatterings"]
         d2h_bytes += 8 * 32 + res["histograms"].nbytes + 16 * len(res["events"])
     barrier()
     e2e_s = time.perf_counter() - t0
 
-    totals = torch.tensor([float(tot["total_scatterings"]), float(tot["trajectories"]), float(e2e_scat)],
+    c = tot["counters"]
+    totals = torch.tensor([float(c["total_scatterings"]), float(c["trajectories"]), float(e2e_scat)],
                           dtype=torch.float64, device="cuda")
-    times = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device="cuda")
+    times = torch.tensor([dev_ms, e2e_s, mix_ms], dtype=torch.float64, device="cuda")
+    mix_totals = torch.tensor([float(mix_tot["counters"]["total_scatterings"]) if mix_tot else 0.0,
+                               float(mix_tot["counters"]["trajectories"]) if mix_tot else 0.0],
+                              dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(totals, op=dist.ReduceOp.SUM)
+        dist.all_reduce(mix_totals, op=dist.ReduceOp.SUM)
         dist.all_reduce(times, op=dist.ReduceOp.MAX)
     dev_s = float(times[0]) * 1e-3
     value = float(totals[0]) / dev_s
     traj_rate = float(totals[1]) / dev_s
     e2e_value = float(totals[2]) / float(times[1])
-    flops = (FLOP_PER_ATTEMPT * tot["rk_attempts"] + FLOP_PER_STEP * tot["rk_steps"] +
-             FLOP_PER_SCATTER * tot["total_scatterings"] + FLOP_PER_TRAJ * tot["trajectories"])
+    flops = (FLOP_PER_ATTEMPT * c["rk_attempts"] + FLOP_PER_STEP * c["rk_steps"] +
+             FLOP_PER_SCATTER * c["total_scatterings"] + FLOP_PER_TRAJ * c["trajectories"])
     achieved = flops / (dev_ms * 1e-3) / 1e12
     line = None
     if rank == 0:
@@ -288,10 +316,25 @@ def run_engine_arm(args):
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak > 0 else None, "traffic": None,
                          "peak_source": "measured in this run: DFMA-chain kernel on all SMs (2 FLOP per FMA)",
-                         "flop_model": "%.0f/attempt + %.0f/step + %.0f/scattering + %.0f/trajectory" % (
+                         "flop_model": "%.1f/attempt + %.1f/step + %.0f/scattering + %.0f/trajectory (counted)" % (
                              FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ)},
             "clocks": clock_info,
         }
+        if mix_tot is not None:
+            mix_s = float(times[2]) * 1e-3
+            err = dms_stats.compare_runs(tot, mix_tot)
+            line["mixed"] = {
+                "value": float(mix_totals[0]) / mix_s, "unit": "scatterings/s",
+                "trajectories_per_s": float(mix_totals[1]) / mix_s, "ms_per_step": float(times[2]) / args.steps,
+                "speedup_vs_fp64": (float(mix_totals[0]) / mix_s) / value,
+                "dtype": "f32 stages/geometry/rates + f64 state, energy, error norm, optical depth, accumulators",
+                "error_vs_fp64": {k: err[k] for k in ("capture_fraction_rel_error", "capture_fraction_sigmas",
+                                                      "radial_chi2", "radial_dof", "radial_p_value",
+                                                      "radial_max_bin_deviation", "evaporation_rate_rel_error",
+                                                      "mean_scatterings_rel_error")},
+                "clocks": mix_clocks,
+                "gpu_launches": args.steps,
+            }
     engine.close()
     if world > 1:
         dist.barrier()
@@ -315,6 +358,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--cpu-baseline-seconds", type=float, default=12.0)
     ap.add_argument("--reference-step-seconds", type=float, default=6.0)
     args = ap.parse_args()

@@ -37,9 +37,12 @@ struct dms_ctx
 	SolarTables tables;
 	void* d_tables = nullptr;
 	DevSolar dsolar{};
+	float* d_tables_f = nullptr;    // FP32 r, G*M, G*M slope for the mixed-precision kernel
 	// points
 	std::vector<PointConstants> points;
 	std::vector<double*> d_grids;
+	std::vector<float*> d_grids_f;  // FP32 image of each rate grid, rebuilt when stale
+	std::vector<char> grid_f_valid;
 	DevPoint* d_points = nullptr;
 	int point_capacity = 0;
 	// accumulators
@@ -141,7 +144,7 @@ int Check_Run_Opts(dms_ctx* ctx, const dms_run_opts* o)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null run options");
 	if(!(o->boundary_radius_rsun >= 1.0) || !std::isfinite(o->boundary_radius_rsun))
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "boundary radius must be at least one solar radius");
-	if(o->precision != DMS_PRECISION_FP64)
+	if(o->precision != DMS_PRECISION_FP64 && o->precision != DMS_PRECISION_MIXED)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "unsupported precision");
 	if(o->threads_per_block != 0 && (o->threads_per_block % 32 != 0 || o->threads_per_block > 128))
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "threads_per_block must be a multiple of 32 up to 128");
@@ -153,7 +156,8 @@ int Check_Run_Opts(dms_ctx* ctx, const dms_run_opts* o)
 int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 {
 	const int threads = o->threads_per_block ? static_cast<int>(o->threads_per_block) : 128;
-	const int max_per_sm = Trajectory_Max_Blocks_Per_SM(threads);
+	const bool mixed = o->precision == DMS_PRECISION_MIXED;
+	const int max_per_sm = mixed ? Trajectory_Mixed_Max_Blocks_Per_SM(threads) : Trajectory_Max_Blocks_Per_SM(threads);
 	if(max_per_sm <= 0)
 		return Fail(ctx, DMS_ERR_CUDA, "trajectory kernel cannot be resident with this block size");
 	int per_sm = o->blocks_per_sm ? static_cast<int>(o->blocks_per_sm) : max_per_sm;
@@ -180,11 +184,28 @@ int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 	p.S = ctx->dsolar;
 	p.points = ctx->d_points;
 	p.n_points = static_cast<int>(ctx->points.size());
+	if(mixed)
+	{
+		for(size_t i = 0; i < ctx->points.size(); i++)
+			if(!ctx->grid_f_valid[i])
+			{
+				const size_t n = static_cast<size_t>(ctx->points[i].grid_n);
+				Launch_To_Float(ctx->d_grids[i], ctx->d_grids_f[i], n * n, ctx->stream);
+				DMS_CUDA(ctx, cudaGetLastError());
+				ctx->grid_f_valid[i] = 1;
+			}
+		p.sf_r = ctx->d_tables_f;
+		p.sf_gm = ctx->d_tables_f + ctx->dsolar.n;
+		p.sf_gm_s = ctx->d_tables_f + 2 * static_cast<size_t>(ctx->dsolar.n);
+	}
 	*ctx->h_cancel = 0;
 	DMS_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), ctx->stream));
 	DMS_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), ctx->stream));
 	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
-	Launch_Trajectories(p, blocks, threads, ctx->stream);
+	if(mixed)
+		Launch_Trajectories_Mixed(p, blocks, threads, ctx->stream);
+	else
+		Launch_Trajectories(p, blocks, threads, ctx->stream);
 	DMS_CUDA(ctx, cudaGetLastError());
 	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
 	const auto start = std::chrono::steady_clock::now();
@@ -283,6 +304,8 @@ void dms_destroy(dms_ctx* ctx)
 	if(ctx->stream)
 		cudaStreamSynchronize(ctx->stream);
 	for(double* g : ctx->d_grids) cudaFree(g);
+	for(float* g : ctx->d_grids_f) cudaFree(g);
+	cudaFree(ctx->d_tables_f);
 	cudaFree(ctx->d_tables);
 	cudaFree(ctx->d_points);
 	cudaFree(ctx->d_counters);
@@ -390,6 +413,24 @@ int dms_load_solar_model(dms_ctx* ctx, const char* path)
 	S.nt_s = dd + offsets[10];
 	S.target_mass = dd + off_mass;
 	S.bucket = reinterpret_cast<const uint16_t*>(dd + off);
+	// FP32 images of the three tables the mixed-precision RK45 stages read
+	std::vector<float> hf(3 * n);
+	for(size_t i = 0; i < n; i++)
+	{
+		hf[i] = static_cast<float>(t.r[i]);
+		hf[n + i] = static_cast<float>(t.gm[i]);
+		hf[2 * n + i] = static_cast<float>(t.gm_s[i]);
+	}
+	float* df = nullptr;
+	DMS_CUDA(ctx, cudaMalloc(&df, sizeof(float) * hf.size()));
+	const cudaError_t cf = cudaMemcpy(df, hf.data(), sizeof(float) * hf.size(), cudaMemcpyHostToDevice);
+	if(cf != cudaSuccess)
+	{
+		cudaFree(df);
+		return Fail(ctx, DMS_ERR_CUDA, std::string("table upload: ") + cudaGetErrorString(cf));
+	}
+	cudaFree(ctx->d_tables_f);
+	ctx->d_tables_f = df;
 	ctx->tables = std::move(t);
 	ctx->has_solar = true;
 	return DMS_OK;
@@ -444,13 +485,22 @@ int dms_add_point(dms_ctx* ctx, const dms_point_params* params, int* point_id)
 	if(rc != DMS_OK)
 		return rc;
 	double* grid = nullptr;
+	float* grid_f = nullptr;
 	DMS_CUDA(ctx, cudaMalloc(&grid, sizeof(double) * c.grid_n * c.grid_n));
+	const cudaError_t e0 = cudaMalloc(&grid_f, sizeof(float) * c.grid_n * c.grid_n);
+	if(e0 != cudaSuccess)
+	{
+		cudaFree(grid);
+		return Fail(ctx, DMS_ERR_CUDA, cudaGetErrorString(e0));
+	}
 	DevPoint d;
 	Fill_Dev_Point(c, grid, d);
+	d.grid_f = grid_f;
 	const cudaError_t e1 = cudaMemcpy(ctx->d_points + id, &d, sizeof d, cudaMemcpyHostToDevice);
 	if(e1 != cudaSuccess)
 	{
 		cudaFree(grid);
+		cudaFree(grid_f);
 		return Fail(ctx, DMS_ERR_CUDA, cudaGetErrorString(e1));
 	}
 	Launch_Rate_Grid(ctx->dsolar, ctx->d_points + id, grid, c.grid_n, ctx->stream);
@@ -458,10 +508,13 @@ int dms_add_point(dms_ctx* ctx, const dms_point_params* params, int* point_id)
 	if(e2 != cudaSuccess || cudaGetLastError() != cudaSuccess)
 	{
 		cudaFree(grid);
+		cudaFree(grid_f);
 		return Fail(ctx, DMS_ERR_CUDA, std::string("rate grid kernel: ") + cudaGetErrorString(e2));
 	}
 	ctx->points.push_back(c);
 	ctx->d_grids.push_back(grid);
+	ctx->d_grids_f.push_back(grid_f);
+	ctx->grid_f_valid.push_back(0);
 	DMS_CUDA(ctx, cudaMemset(ctx->d_counters + static_cast<size_t>(id) * DMS_NUM_COUNTERS, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_hists + static_cast<size_t>(id) * DMS_NUM_HISTS * DMS_NUM_BINS, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_event_count + id, 0, sizeof(unsigned long long)));
@@ -481,6 +534,7 @@ int dms_set_rate_grid(dms_ctx* ctx, int point_id, const double* grid, uint32_t n
 	if(static_cast<int>(n) != ctx->points[point_id].grid_n)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "grid size does not match the point's interpolation_points");
 	DMS_CUDA(ctx, cudaMemcpy(ctx->d_grids[point_id], grid, sizeof(double) * n * n, cudaMemcpyHostToDevice));
+	ctx->grid_f_valid[point_id] = 0;
 	return DMS_OK;
 }
 

@@ -950,26 +950,39 @@ __device__ __forceinline__ bool unit_vector_at_angle(double cos_theta, double ph
 	return true;
 }
 
-// Scatter = Sample_Target + Sample_Target_Velocity + isotropic angle + New_DM_Velocity,
-// src/Simulation_Trajectory.cpp:1122-1269.  Returns false where the reference throws.
-static __device__ __noinline__ bool scatter(const DevSolar& S, const DevPoint* __restrict__ P, Draws& D, Event& e)
+// One channel of Total_DM_Scattering_Rate_Computed (src/Solar_Model.cpp:263-303) at knot
+// interval i, offset dr and temperature T: k < DMS_NUM_TARGETS the isotope k, k ==
+// DMS_NUM_TARGETS the electrons.  Same expressions, in the same order, as rate_computed.
+__device__ __forceinline__ double channel_rate(const DevSolar& S, const DevPoint* __restrict__ P, int i, double dr, double T, double v, int k)
 {
-	const double r = ev_radius(e);
-	const double v = ev_speed(e);
-	if(r > DMS_RSUN_KM)
-		return false;
-	double rates[DMS_NUM_TARGETS];
-	double re;
-	rate_computed(S, P, r, v, rates, &re);
+	if(k == DMS_NUM_TARGETS)
+	{
+		const double ne = __ldg(S.ne + i) + dr * __ldg(S.ne_s + i);
+		return ne * __ldg(&P->sigma_e) * thermal_relative_speed(T, DMS_MELECTRON_GEV, v);
+	}
+	const size_t o = static_cast<size_t>(i) * DMS_NUM_TARGETS + k;
+	const double n = __ldg(S.nt + o) + dr * __ldg(S.nt_s + o);
+	return n * __ldg(&P->sigma_t[k]) * thermal_relative_speed(T, __ldg(S.target_mass + k), v);
+}
+
+constexpr int TARGET_FAILED = -2;
+
+// Sample_Target (src/Simulation_Trajectory.cpp:1122-1158) from the channel rates rates[0..62]
+// (isotopes) and rates[63] (electrons): validation, the total in the reference's order, one
+// uniform draw and the cumulative pick.  Returns -1 for an electron, the isotope index, or
+// TARGET_FAILED where the reference throws.
+__device__ __forceinline__ int pick_target(Draws& D, const double* rates)
+{
+	const double re = rates[DMS_NUM_TARGETS];
 	for(int k = 0; k < DMS_NUM_TARGETS; k++)
 		if(!isfinite(rates[k]) || rates[k] < 0.0)
-			return false;
+			return TARGET_FAILED;
 	if(!isfinite(re) || re < 0.0)
-		return false;
+		return TARGET_FAILED;
 	double total = re;
 	for(int k = 0; k < DMS_NUM_TARGETS; k++) total += rates[k];
 	if(!isfinite(total) || total <= 0.0)
-		return false;
+		return TARGET_FAILED;
 	const double xi = D.uniform(0.0, 1.0);
 	int target = -1;
 	double sum = re / total;
@@ -985,6 +998,15 @@ static __device__ __noinline__ bool scatter(const DevSolar& S, const DevPoint* _
 			}
 		}
 	}
+	return target;
+}
+
+// The rest of Scatter once the target is known: Sample_Target_Velocity, the isotropic
+// scattering angle and New_DM_Velocity, src/Simulation_Trajectory.cpp:1160-1269.  Returns
+// false where the reference throws.
+static __device__ __noinline__ bool scatter_with_target(const DevSolar& S, const DevPoint* __restrict__ P, Draws& D, Event& e, int target)
+{
+	const double r = ev_radius(e);
 	double m_target;
 	if(target < 0)
 		m_target = DMS_MELECTRON_GEV;

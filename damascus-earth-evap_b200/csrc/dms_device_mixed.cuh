@@ -1,0 +1,385 @@
+// Mixed-precision physics of the trajectory engine (the "batched FP32" form).
+//
+// Bulk arithmetic runs in FP32: RK45 stages (with FP32 copies of the G*M table), the 3-D event
+// reconstruction, chord geometry, rate interpolation (FP32 copy of the rate grid) and the
+// scattering kinematics.  FP64 is kept where the precision decides: the propagator's
+// accumulated state (radius, radial speed, angle, time) is FP64 and receives the FP32
+// increments; the RK45 error norm is formed in FP64 from the FP32 stage values (as a direct
+// weighted sum of the stage differences, free of the r5 - r4 cancellation); the orbital energy
+// whose sign decides capture and unbinding, the optical depth still to travel, and the
+// histogram / evaporation accumulators are FP64.  Same algorithm and draw sequence as the FP64
+// form; results agree statistically, not bit for bit.
+#pragma once
+
+#include "dms_device.cuh"
+
+namespace dms
+{
+namespace mixed
+{
+
+struct F3
+{
+	float x, y, z;
+};
+
+__device__ __forceinline__ F3 f3(float a, float b, float c) { return F3{a, b, c}; }
+__device__ __forceinline__ float dotf(const F3& a, const F3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float normf(const F3& a) { return sqrtf(dotf(a, a)); }
+
+// Event with FP64 time and FP32 position / velocity (km, km/s) of one free segment.
+struct EventF
+{
+	double t;
+	F3 x, v;
+};
+
+// Propagator: FP64 accumulators, FP32 orbital-plane frame.
+struct PropF
+{
+	double time, radius, phi, v_radial, time_step;
+	float J;
+	F3 ax, ay;
+	int radial_mode;
+};
+
+// FP32 images of the tables the propagation reads every step.
+struct DevSolarF
+{
+	const float* r;      // knots
+	const float* gm;
+	const float* gm_s;
+};
+
+__device__ __forceinline__ int knot_index_f(const DevSolar& S, const DevSolarF& F, float x)
+{
+	const int last = S.n - 2;
+	if(x >= __ldg(F.r + last))
+		return last;
+	if(!(x >= 0.0f))
+		return 0;
+	int b = static_cast<int>(x * static_cast<float>(S.bucket_scale));
+	b = b > S.nbuckets ? S.nbuckets : b;
+	int i = __ldg(S.bucket + b);
+	while(i > 0 && __ldg(F.r + i) > x) i--;
+	while(i < last && __ldg(F.r + i + 1) <= x) i++;
+	return i;
+}
+
+__device__ __forceinline__ float gm_f(const DevSolar& S, const DevSolarF& F, float r)
+{
+	r = r < 0.0f ? 0.0f : r;
+	if(r > static_cast<float>(DMS_RSUN_KM))
+		return static_cast<float>(DMS_GMSUN_KM3S2);
+	const int i = knot_index_f(S, F, r);
+	return __ldg(F.gm + i) + (r - __ldg(F.r + i)) * __ldg(F.gm_s + i);
+}
+
+// J^2/r^3 - G M/r^2 with one reciprocal
+__device__ __forceinline__ float dv_dt_f(float J, float r, float gm)
+{
+	r = r < 1.0f ? 1.0f : r;
+	const float inv = __frcp_rn(r);
+	return (J * J * inv - gm) * inv * inv;
+}
+
+__device__ __forceinline__ float dphi_dt_f(const PropF& p, float r)
+{
+	if(p.radial_mode || p.J == 0.0f || r <= 0.0f)
+		return 0.0f;
+	const float inv = __frcp_rn(r);
+	return p.J * inv * inv;
+}
+
+// One pass of the Runge_Kutta_45_Step retry loop (src/Simulation_Trajectory.cpp:1492-1600):
+// FP32 stages, FP64 error norm and state update.
+__device__ __forceinline__ int rk45_attempt_f(const DevSolar& S, const DevSolarF& F, PropF& p, int inner)
+{
+	const float dt = static_cast<float>(p.time_step);
+	const float r = static_cast<float>(p.radius), v = static_cast<float>(p.v_radial);
+	const float J = p.J;
+	float kr0, kr1, kr2, kr3, kr4, kr5, kv0, kv1, kv2, kv3, kv4, kv5, kp0, kp2, kp3, kp4, kp5, ri;
+	kr0 = dt * v;
+	kv0 = dt * dv_dt_f(J, r, gm_f(S, F, r));
+	kp0 = dt * dphi_dt_f(p, r);
+	ri = r + 0.25f * kr0;
+	kr1 = dt * (v + 0.25f * kv0);
+	kv1 = dt * dv_dt_f(J, ri, gm_f(S, F, ri));
+	ri = r + (3.0f / 32.0f) * kr0 + (9.0f / 32.0f) * kr1;
+	kr2 = dt * (v + (3.0f / 32.0f) * kv0 + (9.0f / 32.0f) * kv1);
+	kv2 = dt * dv_dt_f(J, ri, gm_f(S, F, ri));
+	kp2 = dt * dphi_dt_f(p, ri);
+	ri = r + (1932.0f / 2197.0f) * kr0 - (7200.0f / 2197.0f) * kr1 + (7296.0f / 2197.0f) * kr2;
+	kr3 = dt * (v + (1932.0f / 2197.0f) * kv0 - (7200.0f / 2197.0f) * kv1 + (7296.0f / 2197.0f) * kv2);
+	kv3 = dt * dv_dt_f(J, ri, gm_f(S, F, ri));
+	kp3 = dt * dphi_dt_f(p, ri);
+	ri = r + (439.0f / 216.0f) * kr0 - 8.0f * kr1 + (3680.0f / 513.0f) * kr2 - (845.0f / 4104.0f) * kr3;
+	kr4 = dt * (v + (439.0f / 216.0f) * kv0 - 8.0f * kv1 + (3680.0f / 513.0f) * kv2 - (845.0f / 4104.0f) * kv3);
+	kv4 = dt * dv_dt_f(J, ri, gm_f(S, F, ri));
+	kp4 = dt * dphi_dt_f(p, ri);
+	ri = r - (8.0f / 27.0f) * kr0 + 2.0f * kr1 - (3544.0f / 2565.0f) * kr2 + (1859.0f / 4104.0f) * kr3 - (11.0f / 40.0f) * kr4;
+	kr5 = dt * (v - (8.0f / 27.0f) * kv0 + 2.0f * kv1 - (3544.0f / 2565.0f) * kv2 + (1859.0f / 4104.0f) * kv3 - (11.0f / 40.0f) * kv4);
+	kv5 = dt * dv_dt_f(J, ri, gm_f(S, F, ri));
+	kp5 = dt * dphi_dt_f(p, ri);
+	// 4th-order increments (FP32) and the 5th - 4th order difference in FP64
+	const float dr4 = (25.0f / 216.0f) * kr0 + (1408.0f / 2565.0f) * kr2 + (2197.0f / 4104.0f) * kr3 - 0.2f * kr4;
+	const float dv4 = (25.0f / 216.0f) * kv0 + (1408.0f / 2565.0f) * kv2 + (2197.0f / 4104.0f) * kv3 - 0.2f * kv4;
+	const float dp4 = (25.0f / 216.0f) * kp0 + (1408.0f / 2565.0f) * kp2 + (2197.0f / 4104.0f) * kp3 - 0.2f * kp4;
+	// (b5 - b4): 16/135 - 25/216, 0, 6656/12825 - 1408/2565, 28561/56430 - 2197/4104, -9/50 + 1/5, 2/55
+	const double c0 = 16.0 / 135.0 - 25.0 / 216.0, c2 = 6656.0 / 12825.0 - 1408.0 / 2565.0, c3 = 28561.0 / 56430.0 - 2197.0 / 4104.0,
+	             c4 = -9.0 / 50.0 + 1.0 / 5.0, c5 = 2.0 / 55.0;
+	const double e0 = fabs(c0 * kr0 + c2 * kr2 + c3 * kr3 + c4 * kr4 + c5 * kr5);
+	const double e1 = fabs(c0 * kv0 + c2 * kv2 + c3 * kv3 + c4 * kv4 + c5 * kv5);
+	const double e2 = fabs(c0 * kp0 + c2 * kp2 + c3 * kp3 + c4 * kp4 + c5 * kp5);
+	const bool finite_state = isfinite(dr4) && isfinite(dv4) && isfinite(dp4);
+	// RK45_Next_Step_Size, src/Simulation_Trajectory.cpp:477-502
+	double new_step;
+	if(!isfinite(e0) || !isfinite(e1) || !isfinite(e2))
+		new_step = DMS_RK45_MIN_STEP_FACTOR * p.time_step;
+	else
+	{
+		float factor = static_cast<float>(DMS_RK45_MAX_STEP_FACTOR), c;
+		if(e0 > 0.0)
+		{
+			c = 0.84f * sqrtf(sqrtf(static_cast<float>(DMS_RK45_TOL_R_KM / e0)));
+			if(isfinite(c) && c < factor) factor = c;
+		}
+		if(e1 > 0.0)
+		{
+			c = 0.84f * sqrtf(sqrtf(static_cast<float>(DMS_RK45_TOL_V_KMS / e1)));
+			if(isfinite(c) && c < factor) factor = c;
+		}
+		if(e2 > 0.0)
+		{
+			c = 0.84f * sqrtf(sqrtf(static_cast<float>(DMS_RK45_TOL_PHI / e2)));
+			if(isfinite(c) && c < factor) factor = c;
+		}
+		factor = factor < static_cast<float>(DMS_RK45_MIN_STEP_FACTOR) ? static_cast<float>(DMS_RK45_MIN_STEP_FACTOR) : factor;
+		new_step = sanitized_step(static_cast<double>(factor) * p.time_step);
+	}
+	const bool within = isfinite(e0) && e0 <= DMS_RK45_TOL_R_KM && isfinite(e1) && e1 <= DMS_RK45_TOL_V_KMS && isfinite(e2) && e2 <= DMS_RK45_TOL_PHI;
+	if(within)
+	{
+		p.time = p.time + p.time_step;
+		const double r4 = p.radius + static_cast<double>(dr4);
+		p.radius = r4 < 0.0 ? 0.0 : r4;
+		p.v_radial = p.v_radial + static_cast<double>(dv4);
+		p.phi = p.phi + static_cast<double>(dp4);
+		p.time_step = new_step;
+		return RK_ACCEPTED;
+	}
+	if(new_step < DMS_RK45_ABS_MIN_STEP_S || inner >= DMS_RK45_MAX_INNER_RETRIES)
+	{
+		p.time = p.time + DMS_RK45_ABS_MIN_STEP_S;
+		if(finite_state)
+		{
+			const double r4 = p.radius + static_cast<double>(dr4);
+			p.radius = r4 < 0.0 ? 0.0 : r4;
+			p.v_radial = p.v_radial + static_cast<double>(dv4);
+			p.phi = p.phi + static_cast<double>(dp4);
+		}
+		p.time_step = DMS_RK45_ABS_MIN_STEP_S;
+		return RK_FORCED;
+	}
+	p.time_step = new_step;
+	return RK_RETRY;
+}
+
+__device__ __forceinline__ double prop_radius_f(const PropF& p) { return p.radius < 0.0 ? 0.0 : p.radius; }
+
+__device__ __forceinline__ double prop_speed_f(const PropF& p)
+{
+	const double r = p.radius < 0.0 ? 0.0 : p.radius;
+	if(r == 0 || p.J == 0.0f)
+		return fabs(p.v_radial);
+	const double vt = static_cast<double>(p.J) / r;
+	return sqrt(p.v_radial * p.v_radial + vt * vt);
+}
+
+// Event_In_3D (src/Simulation_Trajectory.cpp:1715-1742) with the angle reduced in FP64 first
+__device__ __forceinline__ EventF prop_event_f(const PropF& p)
+{
+	const double safe = (isfinite(p.radius) && p.radius > 0.0) ? p.radius : 0.0;
+	EventF e;
+	e.t = p.time;
+	const float sr = static_cast<float>(safe), vr = static_cast<float>(p.v_radial);
+	if(p.radial_mode || p.J == 0.0f || safe == 0.0)
+	{
+		e.x = f3(sr * p.ax.x, sr * p.ax.y, sr * p.ax.z);
+		e.v = f3(vr * p.ax.x, vr * p.ax.y, vr * p.ax.z);
+		return e;
+	}
+	const double turns = rint(p.phi * (1.0 / (2.0 * DMS_PI)));
+	const float phi = static_cast<float>(p.phi - turns * (2.0 * DMS_PI));
+	float sp, cp;
+	sincosf(phi, &sp, &cp);
+	const float vt = p.J / sr;
+	const float vx = vr * cp - vt * sp;
+	const float vy = vr * sp + vt * cp;
+	e.x = f3(sr * (cp * p.ax.x + sp * p.ay.x), sr * (cp * p.ax.y + sp * p.ay.y), sr * (cp * p.ax.z + sp * p.ay.z));
+	e.v = f3(vx * p.ax.x + vy * p.ay.x, vx * p.ax.y + vy * p.ay.y, vx * p.ax.z + vy * p.ay.z);
+	return e;
+}
+
+// Free_Particle_Propagator constructor from an FP64 event (frame in FP32)
+__device__ __forceinline__ void prop_init_f(PropF& q, const Event& e)
+{
+	Prop p;
+	prop_init(p, e);
+	q.time = p.time;
+	q.radius = p.radius;
+	q.phi = p.phi;
+	q.v_radial = p.v_radial;
+	q.time_step = p.time_step;
+	q.J = static_cast<float>(p.J);
+	q.ax = f3(static_cast<float>(p.ax.x), static_cast<float>(p.ax.y), static_cast<float>(p.ax.z));
+	q.ay = f3(static_cast<float>(p.ay.x), static_cast<float>(p.ay.y), static_cast<float>(p.ay.z));
+	q.radial_mode = p.radial_mode;
+}
+
+__device__ __forceinline__ Event to_event64(const EventF& e)
+{
+	Event o;
+	o.t = e.t;
+	o.x = mk(e.x.x, e.x.y, e.x.z);
+	o.v = mk(e.v.x, e.v.y, e.v.z);
+	return o;
+}
+
+// Total_DM_Scattering_Rate through the FP32 copy of the grid (src/Solar_Model.cpp:344-393);
+// speeds above the grid fall back to the FP64 direct sum as in the reference.
+__device__ __forceinline__ float rate_total_f(const DevSolar& S, const DevPoint* __restrict__ P, const float* __restrict__ grid, float r, float v)
+{
+	if(!isfinite(r) || !isfinite(v))
+		return NAN;
+	r = r < 0.0f ? 0.0f : r;
+	v = v < 0.0f ? 0.0f : v;
+	if(!(v <= static_cast<float>(__ldg(&P->grid_vmax))))
+		return static_cast<float>(rate_computed(S, P, r, v, nullptr, nullptr));
+	if(r > static_cast<float>(DMS_RSUN_KM))
+		return 0.0f;
+	const float rc = r * static_cast<float>(__ldg(&P->grid_inv_r));
+	const float vc = v * static_cast<float>(__ldg(&P->grid_inv_v));
+	const unsigned int N = static_cast<unsigned int>(__ldg(&P->grid_n));
+	unsigned int ri = static_cast<unsigned int>(rc);
+	unsigned int vi = static_cast<unsigned int>(vc);
+	ri = ri > N - 2 ? N - 2 : ri;
+	vi = vi > N - 2 ? N - 2 : vi;
+	const float rf = rc - ri, vf = vc - vi;
+	const size_t lower = static_cast<size_t>(ri) * N + vi;
+	const float g00 = __ldg(grid + lower), g01 = __ldg(grid + lower + 1);
+	const float g10 = __ldg(grid + lower + N), g11 = __ldg(grid + lower + N + 1);
+	const float lo = g00 + vf * (g01 - g00);
+	const float hi = g10 + vf * (g11 - g10);
+	const float rate = lo + rf * (hi - lo);
+	return isfinite(rate) ? (rate > 0.0f ? rate : 0.0f) : NAN;
+}
+
+__device__ __forceinline__ float rate_at_fraction_f(const DevSolar& S, const DevPoint* __restrict__ P, const float* __restrict__ grid,
+                                                    const EventF& a, const EventF& b, float f)
+{
+	f = f < 0.0f ? 0.0f : (f > 1.0f ? 1.0f : f);
+	const float x = a.x.x + f * (b.x.x - a.x.x), vx = a.v.x + f * (b.v.x - a.v.x);
+	const float y = a.x.y + f * (b.x.y - a.x.y), vy = a.v.y + f * (b.v.y - a.v.y);
+	const float z = a.x.z + f * (b.x.z - a.x.z), vz = a.v.z + f * (b.v.z - a.v.z);
+	const float r = sqrtf(fmaxf(x * x + y * y + z * z, 0.0f));
+	if(r >= static_cast<float>(DMS_RSUN_KM))
+		return 0.0f;
+	return rate_total_f(S, P, grid, r, sqrtf(fmaxf(vx * vx + vy * vy + vz * vz, 0.0f)));
+}
+
+__device__ __forceinline__ float radius_at_fraction_f(const EventF& a, const EventF& b, float f)
+{
+	f = f < 0.0f ? 0.0f : (f > 1.0f ? 1.0f : f);
+	const float x = a.x.x + f * (b.x.x - a.x.x), y = a.x.y + f * (b.x.y - a.x.y), z = a.x.z + f * (b.x.z - a.x.z);
+	return sqrtf(fmaxf(x * x + y * y + z * z, 0.0f));
+}
+
+// Solar_Interior_Fraction_Interval (src/Simulation_Trajectory.cpp:231-325); the quadratic's
+// constant term |x|^2 - R^2 is formed in FP64 to avoid cancellation near the surface
+__device__ __forceinline__ bool interior_interval_f(const EventF& a, const EventF& b, double ra, double rb, float& start, float& end)
+{
+	const bool a_in = ra < DMS_RSUN_KM, b_in = rb < DMS_RSUN_KM;
+	const float dx = b.x.x - a.x.x, dy = b.x.y - a.x.y, dz = b.x.z - a.x.z;
+	const double qa = static_cast<double>(dx * dx + dy * dy + dz * dz);
+	const double qb = 2.0 * static_cast<double>(a.x.x * dx + a.x.y * dy + a.x.z * dz);
+	const double ax = a.x.x, ay = a.x.y, az = a.x.z;
+	const double qc = (ax * ax + ay * ay + az * az) - DMS_RSUN_KM * DMS_RSUN_KM;
+	bool has = false;
+	float c1 = 0.0f, c2 = 0.0f;
+	if(qa > 0.0)
+	{
+		const double disc = qb * qb - 4.0 * qa * qc;
+		if(isfinite(disc) && disc >= 0.0)
+		{
+			const double sq = sqrt(disc);
+			double f1 = (-qb - sq) / (2.0 * qa), f2 = (-qb + sq) / (2.0 * qa);
+			if(f1 > f2)
+			{
+				const double t = f1;
+				f1 = f2;
+				f2 = t;
+			}
+			c1 = static_cast<float>(f1);
+			c2 = static_cast<float>(f2);
+			has = true;
+		}
+	}
+	auto in_unit_f = [](float f) { return f >= -1.0e-12f && f <= 1.0f + 1.0e-6f; };
+	auto clampf = [](float f) { return f < 0.0f ? 0.0f : (f > 1.0f ? 1.0f : f); };
+	auto bisect = [&]() {
+		float lower = 0.0f, upper = 1.0f;
+		float r_lower = radius_at_fraction_f(a, b, lower) - static_cast<float>(DMS_RSUN_KM);
+		for(int it = 0; it < 30; it++)
+		{
+			const float mid = 0.5f * (lower + upper);
+			const float r_mid = radius_at_fraction_f(a, b, mid) - static_cast<float>(DMS_RSUN_KM);
+			if((r_lower <= 0.0f && r_mid <= 0.0f) || (r_lower >= 0.0f && r_mid >= 0.0f))
+			{
+				lower = mid;
+				r_lower = r_mid;
+			}
+			else
+				upper = mid;
+		}
+		return clampf(0.5f * (lower + upper));
+	};
+	if(a_in && b_in)
+	{
+		start = 0.0f;
+		end = 1.0f;
+		return true;
+	}
+	if(!a_in && b_in)
+	{
+		start = (has && in_unit_f(c1)) ? clampf(c1) : (has && in_unit_f(c2)) ? clampf(c2) : bisect();
+		end = 1.0f;
+		return end > start;
+	}
+	if(a_in && !b_in)
+	{
+		start = 0.0f;
+		end = (has && in_unit_f(c2)) ? clampf(c2) : (has && in_unit_f(c1)) ? clampf(c1) : bisect();
+		return end > start;
+	}
+	if(has && in_unit_f(c1) && in_unit_f(c2))
+	{
+		start = clampf(c1);
+		end = clampf(c2);
+		return end > start;
+	}
+	return false;
+}
+
+__device__ __forceinline__ EventF interpolate_event_f(const EventF& a, const EventF& b, float f)
+{
+	f = f < 0.0f ? 0.0f : (f > 1.0f ? 1.0f : f);
+	EventF e;
+	e.x = f3(a.x.x + f * (b.x.x - a.x.x), a.x.y + f * (b.x.y - a.x.y), a.x.z + f * (b.x.z - a.x.z));
+	e.v = f3(a.v.x + f * (b.v.x - a.v.x), a.v.y + f * (b.v.y - a.v.y), a.v.z + f * (b.v.z - a.v.z));
+	e.t = a.t + static_cast<double>(f) * (b.t - a.t);
+	return e;
+}
+
+}	// namespace mixed
+}	// namespace dms

@@ -317,27 +317,7 @@ __device__ __forceinline__ int free_step(const RunParams& R, const DevPoint* __r
 			L.reason = DMS_REASON_SCATTER;
 			return PH_FINAL;
 		}
-		if(!scatter(S, P, L.D, L.cur))
-		{
-			L.reason = DMS_REASON_NUMERICAL_FAILURE;
-			return PH_FINAL;
-		}
-		L.nscat++;
-		const bool captured = update_capture_state(S, m_dm, capture_mode, L, ev_radius(L.cur), ev_speed(L.cur), L.cur.t, true);
-		if(!capture_mode)
-		{
-			// Reset_Bincount_Anchor, src/Simulation_Trajectory.cpp:671-680
-			L.prev_time = L.cur.t;
-			L.prev_r = ev_radius(L.cur);
-			const double v = ev_speed(L.cur);
-			L.prev_v2 = v * v;
-		}
-		if(capture_mode && captured)
-		{
-			L.reason = DMS_REASON_CAPTURE_MODE;
-			return PH_FINAL;
-		}
-		return PH_SEGMENT;
+		return PH_SCATTER;  // Sample_Target runs warp-cooperatively in the lane loop
 	}
 	L.before = after;
 	return PH_STEP;

@@ -17,6 +17,7 @@ enum Phase : int
 	PH_STEP = 2,
 	PH_FINAL = 3,
 	PH_DONE = 4,
+	PH_SCATTER = 5,  // the committed event L.cur is a scattering point inside the Sun
 };
 
 
@@ -456,11 +457,83 @@ __device__ __forceinline__ int start_trajectory(const RunParams& R, Lane& L, uin
 	return PH_SEGMENT;
 }
 
+// Sample_Target for every lane of the converged group that is at a scattering point.  The 64
+// channel rates of one scattering lane (63 isotopes + electrons, the dominant cost of a
+// scatter) are evaluated by all lanes of the group in parallel into shared memory; the
+// scattering lane then validates, sums and picks sequentially in the reference's order, so
+// the target and the draws consumed are those of the one-lane form.  `rates` is this warp's
+// DMS_NUM_TARGETS + 1 doubles of shared memory.
+template <class Lane>
+__device__ __forceinline__ void cooperative_targets(const RunParams& R, Lane& L, int phase, double* rates, int& target)
+{
+	const unsigned int grp = __activemask();
+	unsigned int pending = __ballot_sync(grp, phase == PH_SCATTER);
+	if(pending == 0u)
+		return;
+	const int me = threadIdx.x & 31;
+	const int rank = __popc(grp & ((1u << me) - 1u));
+	const int size = __popc(grp);
+	const bool mine = phase == PH_SCATTER;
+	const double my_r = mine ? ev_radius(L.cur) : 0.0;
+	const double my_v = mine ? ev_speed(L.cur) : 0.0;
+	while(pending != 0u)
+	{
+		const int leader = __ffs(pending) - 1;
+		pending &= pending - 1u;
+		const double r = __shfl_sync(grp, my_r, leader);
+		const double v = __shfl_sync(grp, my_v, leader);
+		const int point = __shfl_sync(grp, L.point, leader);
+		if(isfinite(r) && isfinite(v))
+		{
+			const DevPoint* P = R.points + point;
+			const int i = knot_index(R.S, r);
+			const double dr = r - __ldg(R.S.r + i);
+			const double T = __ldg(R.S.temp + i) + dr * __ldg(R.S.temp_s + i);
+			for(int k = rank; k <= DMS_NUM_TARGETS; k += size)
+				rates[k] = channel_rate(R.S, P, i, dr, T, v, k);
+		}
+		__syncwarp(grp);
+		if(me == leader)
+			target = (isfinite(r) && isfinite(v)) ? pick_target(L.D, rates) : TARGET_FAILED;
+		__syncwarp(grp);
+	}
+}
+
+// Simulate after a scattering point (src/Simulation_Trajectory.cpp:1313-1346): target
+// velocity, angle and kinematics, then capture bookkeeping and the bincount anchor.
+template <class Lane>
+__device__ __forceinline__ int finish_scatter(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, Lane& L, int target)
+{
+	if(target == TARGET_FAILED || !scatter_with_target(R.S, P, L.D, L.cur, target))
+	{
+		L.reason = DMS_REASON_NUMERICAL_FAILURE;
+		return PH_FINAL;
+	}
+	L.nscat++;
+	const bool captured = update_capture_state(R.S, m_dm, R.capture_mode, L, ev_radius(L.cur), ev_speed(L.cur), L.cur.t, true);
+	if(!R.capture_mode)
+	{
+		// Reset_Bincount_Anchor, src/Simulation_Trajectory.cpp:671-680
+		L.prev_time = L.cur.t;
+		L.prev_r = ev_radius(L.cur);
+		const double v = ev_speed(L.cur);
+		L.prev_v2 = v * v;
+	}
+	if(R.capture_mode && captured)
+	{
+		L.reason = DMS_REASON_CAPTURE_MODE;
+		return PH_FINAL;
+	}
+	return PH_SEGMENT;
+}
+
 template <class Lane, class Step>
 __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 {
 	const int lane_id = blockIdx.x * blockDim.x + threadIdx.x;
 	double2* hist = R.lane_hist + static_cast<size_t>(lane_id) * DMS_NUM_BINS;
+	__shared__ double coop_rates[4][DMS_NUM_TARGETS + 1];  // blocks of at most 128 threads
+	double* rates = coop_rates[threadIdx.x >> 5];
 	Lane L;
 	const DevPoint* P = R.points;
 	double m_dm = 0.0;
@@ -500,6 +573,10 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 			phase = segment_start(R, P, m_dm, L);
 		if(phase == PH_STEP)
 			phase = step(R, P, m_dm, L, hist);
+		int target = TARGET_FAILED;
+		cooperative_targets(R, L, phase, rates, target);
+		if(phase == PH_SCATTER)
+			phase = finish_scatter(R, P, m_dm, L, target);
 		if(phase == PH_FINAL)
 		{
 			finalize(R, P, m_dm, L, hist);

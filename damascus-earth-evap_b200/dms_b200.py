@@ -114,8 +114,12 @@ def library():
     return lib
 
 
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+
 def run_opts(seed=1, capture_mode=False, max_scatterings=10 ** 14, max_free_steps=10 ** 12, boundary_rsun=2.0,
-             threads_per_block=0, blocks_per_sm=0, time_limit_s=0.0, iteration_budget=0):
+             threads_per_block=0, blocks_per_sm=0, time_limit_s=0.0, iteration_budget=0, precision=PRECISION_FP64):
     o = RunOpts()
     library().dms_default_run_opts(ctypes.byref(o))
     o.seed = seed
@@ -127,6 +131,7 @@ def run_opts(seed=1, capture_mode=False, max_scatterings=10 ** 14, max_free_step
     o.blocks_per_sm = blocks_per_sm
     o.time_limit_s = time_limit_s
     o.iteration_budget = iteration_budget
+    o.precision = precision
     return o
 
 

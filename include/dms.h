@@ -150,7 +150,13 @@ int dms_get_rate_grid(dms_ctx* ctx, int point_id, double* grid, uint32_t n);
 int dms_rate(dms_ctx* ctx, int point_id, int interpolated, const double* r_km, const double* v_kms, double* rate_out, size_t n);
 
 /* ---- runs -------------------------------------------------------------------------------- */
+/* FP64: every operation in the reference's FP64 order (bit-identical with the CPU oracle).
+ * MIXED: the batched FP32 form (no reference counterpart; the reference is FP64 only): RK45
+ * stages, the 3-D event, chord geometry and rate interpolation in FP32; propagator state,
+ * time, optical depth, orbital energy, the RK45 error norm, scattering kinematics and the
+ * accumulators in FP64.  Agrees with FP64 statistically, not trajectory by trajectory. */
 #define DMS_PRECISION_FP64  0
+#define DMS_PRECISION_MIXED 1
 
 typedef struct
 {
