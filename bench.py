@@ -351,6 +351,25 @@ def run_engine_arm(args):
         print(json.dumps(line), flush=True)
 
 
+def run_profile_case(args):
+    """One trajectory launch for a profiler (no timing, no JSON line): `single` runs trajectory
+    id 1612 alone (the longest of ids 0..16383 of this point, 38944 accepted steps in the FP64
+    form: the per-lane latency of the tail), `saturated` runs 2^19 trajectories (about seven per
+    resident lane: the bulk throughput), `step` runs one bench step (65536 trajectories)."""
+    import dms_b200
+    prec = dms_b200.PRECISION_MIXED if args.precision == "mixed" else dms_b200.PRECISION_FP64
+    engine = dms_b200.Engine(0)
+    pid = engine.add_point(dms_b200.point_params(MASS_GEV, SIGMA_CM2, interpolation_points=GRID_N))
+    opts = dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT, time_limit_s=300.0, precision=prec)
+    first, count = {"single": (1612, 1), "saturated": (0, 1 << 19), "step": (0, TRAJECTORIES)}[args.profile_case]
+    engine.run([(pid, first, count)], opts)
+    c = engine.results(pid, events_capacity=1)["counters"]
+    print(json.dumps({"profile_case": args.profile_case, "precision": args.precision, "kernel_ms": engine.last_kernel_ms(),
+                      "trajectories": c["trajectories"], "rk_steps": c["rk_steps"], "rk_attempts": c["rk_attempts"],
+                      "scatterings": c["total_scatterings"]}), flush=True)
+    engine.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -361,8 +380,13 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--cpu-baseline-seconds", type=float, default=12.0)
     ap.add_argument("--reference-step-seconds", type=float, default=6.0)
+    ap.add_argument("--profile-case", choices=["single", "saturated", "step"],
+                    help="run one trajectory launch for a profiler and exit")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64", help="form used by --profile-case")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_engine_arm(args)

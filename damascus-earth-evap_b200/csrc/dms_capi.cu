@@ -54,6 +54,8 @@ struct dms_ctx
 	// run scratch
 	double2* d_lane_hist = nullptr;
 	size_t lane_capacity = 0;
+	InitState* d_init = nullptr;    // initial state of every work index of a launch
+	uint64_t init_capacity = 0;
 	unsigned long long* d_queue = nullptr;
 	unsigned int* d_status = nullptr;
 	int* h_cancel = nullptr;       // mapped host memory
@@ -138,6 +140,19 @@ int Ensure_Lanes(dms_ctx* ctx, size_t lanes)
 	return DMS_OK;
 }
 
+int Ensure_Init(dms_ctx* ctx, uint64_t total)
+{
+	if(total <= ctx->init_capacity)
+		return DMS_OK;
+	cudaFree(ctx->d_init);
+	ctx->d_init = nullptr;
+	ctx->init_capacity = 0;
+	const uint64_t cap = std::max<uint64_t>(total, 1 << 16);
+	DMS_CUDA(ctx, cudaMalloc(&ctx->d_init, sizeof(InitState) * cap));
+	ctx->init_capacity = cap;
+	return DMS_OK;
+}
+
 int Check_Run_Opts(dms_ctx* ctx, const dms_run_opts* o)
 {
 	if(!o)
@@ -170,7 +185,11 @@ int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 	int rc = Ensure_Lanes(ctx, lanes);
 	if(rc != DMS_OK)
 		return rc;
+	rc = Ensure_Init(ctx, p.total);
+	if(rc != DMS_OK)
+		return rc;
 	p.lane_hist = ctx->d_lane_hist;
+	p.init = ctx->d_init;
 	p.queue_head = ctx->d_queue;
 	p.status = ctx->d_status;
 	p.cancel = ctx->d_cancel;
@@ -197,11 +216,15 @@ int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 		p.sf_r = ctx->d_tables_f;
 		p.sf_gm = ctx->d_tables_f + ctx->dsolar.n;
 		p.sf_gm_s = ctx->d_tables_f + 2 * static_cast<size_t>(ctx->dsolar.n);
+		p.sf_vesc2 = ctx->d_tables_f + 3 * static_cast<size_t>(ctx->dsolar.n);
+		p.sf_vesc2_s = ctx->d_tables_f + 4 * static_cast<size_t>(ctx->dsolar.n);
 	}
 	*ctx->h_cancel = 0;
 	DMS_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), ctx->stream));
 	DMS_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), ctx->stream));
 	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+	Launch_Initial_States(p, ctx->stream);
+	DMS_CUDA(ctx, cudaGetLastError());
 	if(mixed)
 		Launch_Trajectories_Mixed(p, blocks, threads, ctx->stream);
 	else
@@ -305,6 +328,7 @@ void dms_destroy(dms_ctx* ctx)
 		cudaStreamSynchronize(ctx->stream);
 	for(double* g : ctx->d_grids) cudaFree(g);
 	for(float* g : ctx->d_grids_f) cudaFree(g);
+	cudaFree(ctx->d_init);
 	cudaFree(ctx->d_tables_f);
 	cudaFree(ctx->d_tables);
 	cudaFree(ctx->d_points);
@@ -413,13 +437,16 @@ int dms_load_solar_model(dms_ctx* ctx, const char* path)
 	S.nt_s = dd + offsets[10];
 	S.target_mass = dd + off_mass;
 	S.bucket = reinterpret_cast<const uint16_t*>(dd + off);
-	// FP32 images of the three tables the mixed-precision RK45 stages read
-	std::vector<float> hf(3 * n);
+	// FP32 images of the tables the mixed-precision kernel reads every step: knots, G*M and
+	// v_esc^2 with their slopes
+	std::vector<float> hf(5 * n);
 	for(size_t i = 0; i < n; i++)
 	{
 		hf[i] = static_cast<float>(t.r[i]);
 		hf[n + i] = static_cast<float>(t.gm[i]);
 		hf[2 * n + i] = static_cast<float>(t.gm_s[i]);
+		hf[3 * n + i] = static_cast<float>(t.vesc2[i]);
+		hf[4 * n + i] = static_cast<float>(t.vesc2_s[i]);
 	}
 	float* df = nullptr;
 	DMS_CUDA(ctx, cudaMalloc(&df, sizeof(float) * hf.size()));
@@ -756,14 +783,16 @@ int dms_reset_results(dms_ctx* ctx, int point_id)
 // holds these 4 MiB until the process exits.
 //
 // Scratch layout (bytes): 0 work-queue head (u64), 8 status word (u32), 64 range start (u64),
-// 72 range offsets {0, count} (2 x u64), 96 range point (i32); from 256 one 2000-bin
-// (dt, v2dt) histogram row per lane, DMS_NOALLOC_MAX_TRAJECTORIES rows.
+// 72 range offsets {0, count} (2 x u64), 96 range point (i32); from 256 the initial states
+// (64 bytes per trajectory); after them one 2000-bin (dt, v2dt) histogram row per lane,
+// DMS_NOALLOC_MAX_TRAJECTORIES of each.
 static __device__ __align__(256) unsigned char dms_noalloc_scratch[DMS_NOALLOC_SCRATCH_BYTES];
 
 namespace
 {
 constexpr size_t NOALLOC_HEADER = 256;
-static_assert(DMS_NOALLOC_SCRATCH_BYTES == NOALLOC_HEADER + sizeof(double2) * DMS_NUM_BINS * DMS_NOALLOC_MAX_TRAJECTORIES,
+constexpr size_t NOALLOC_ROWS = NOALLOC_HEADER + sizeof(InitState) * DMS_NOALLOC_MAX_TRAJECTORIES;
+static_assert(DMS_NOALLOC_SCRATCH_BYTES == NOALLOC_ROWS + sizeof(double2) * DMS_NUM_BINS * DMS_NOALLOC_MAX_TRAJECTORIES,
               "scratch size must match its layout");
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
@@ -805,7 +834,7 @@ __global__ void noalloc_prepare_kernel(unsigned char* scratch, uint64_t first, u
 		reinterpret_cast<uint64_t*>(scratch + 72)[1] = count;
 		*reinterpret_cast<int32_t*>(scratch + 96) = point;
 	}
-	double2* rows = reinterpret_cast<double2*>(scratch + NOALLOC_HEADER);
+	double2* rows = reinterpret_cast<double2*>(scratch + NOALLOC_ROWS);
 	for(uint64_t k = tid; k < lanes * DMS_NUM_BINS; k += stride) rows[k] = make_double2(0.0, 0.0);
 	for(uint64_t k = tid; k < count * sizeof(dms_traj_record); k += stride) records[k] = 0;
 	if(hist_dt != nullptr)
@@ -857,7 +886,8 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 	p.total = count;
 	p.queue_head = reinterpret_cast<unsigned long long*>(scratch + 0);
 	p.status = reinterpret_cast<unsigned int*>(scratch + 8);
-	p.lane_hist = reinterpret_cast<double2*>(scratch + NOALLOC_HEADER);
+	p.lane_hist = reinterpret_cast<double2*>(scratch + NOALLOC_ROWS);
+	p.init = reinterpret_cast<InitState*>(scratch + NOALLOC_HEADER);
 	p.seed = opts->seed;
 	p.capture_mode = opts->capture_mode ? 1 : 0;
 	p.max_scatterings = opts->max_scatterings;
@@ -880,6 +910,8 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 	                                                   d_hist_dt, d_hist_v2dt);
 	DMS_CUDA(ctx, cudaGetLastError());
 	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+	Launch_Initial_States(p, ctx->stream);
+	DMS_CUDA(ctx, cudaGetLastError());
 	Launch_Trajectories(p, blocks, threads, ctx->stream);
 	DMS_CUDA(ctx, cudaGetLastError());
 	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));

@@ -826,14 +826,14 @@ static __device__ __noinline__ double find_crossing(const Event& a, const Event&
 __device__ __forceinline__ bool interior_interval(const Event& a, const Event& b, double ra, double rb, double& start, double& end)
 {
 	const bool a_in = ra < DMS_RSUN_KM, b_in = rb < DMS_RSUN_KM;
-	double c1 = 0.0, c2 = 0.0;
-	const bool has = surface_crossings(a, b, c1, c2);
 	if(a_in && b_in)
 	{
 		start = 0.0;
 		end = 1.0;
 		return true;
 	}
+	double c1 = 0.0, c2 = 0.0;  // the crossings matter only when a chord end is outside
+	const bool has = surface_crossings(a, b, c1, c2);
 	if(!a_in && b_in)
 	{
 		if(has && in_unit(c1))

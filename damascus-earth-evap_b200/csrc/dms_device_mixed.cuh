@@ -49,6 +49,8 @@ struct DevSolarF
 	const float* r;      // knots
 	const float* gm;
 	const float* gm_s;
+	const float* vesc2;
+	const float* vesc2_s;
 };
 
 __device__ __forceinline__ int knot_index_f(const DevSolar& S, const DevSolarF& F, float x)
@@ -141,17 +143,17 @@ __device__ __forceinline__ int rk45_attempt_f(const DevSolar& S, const DevSolarF
 		float factor = static_cast<float>(DMS_RK45_MAX_STEP_FACTOR), c;
 		if(e0 > 0.0)
 		{
-			c = 0.84f * sqrtf(sqrtf(static_cast<float>(DMS_RK45_TOL_R_KM / e0)));
+			c = 0.84f * sqrtf(sqrtf(static_cast<float>(DMS_RK45_TOL_R_KM) / static_cast<float>(e0)));
 			if(isfinite(c) && c < factor) factor = c;
 		}
 		if(e1 > 0.0)
 		{
-			c = 0.84f * sqrtf(sqrtf(static_cast<float>(DMS_RK45_TOL_V_KMS / e1)));
+			c = 0.84f * sqrtf(sqrtf(static_cast<float>(DMS_RK45_TOL_V_KMS) / static_cast<float>(e1)));
 			if(isfinite(c) && c < factor) factor = c;
 		}
 		if(e2 > 0.0)
 		{
-			c = 0.84f * sqrtf(sqrtf(static_cast<float>(DMS_RK45_TOL_PHI / e2)));
+			c = 0.84f * sqrtf(sqrtf(static_cast<float>(DMS_RK45_TOL_PHI) / static_cast<float>(e2)));
 			if(isfinite(c) && c < factor) factor = c;
 		}
 		factor = factor < static_cast<float>(DMS_RK45_MIN_STEP_FACTOR) ? static_cast<float>(DMS_RK45_MIN_STEP_FACTOR) : factor;
@@ -189,11 +191,30 @@ __device__ __forceinline__ double prop_radius_f(const PropF& p) { return p.radiu
 
 __device__ __forceinline__ double prop_speed_f(const PropF& p)
 {
-	const double r = p.radius < 0.0 ? 0.0 : p.radius;
-	if(r == 0 || p.J == 0.0f)
+	const float r = static_cast<float>(p.radius < 0.0 ? 0.0 : p.radius);
+	const float vr = static_cast<float>(p.v_radial);
+	if(r == 0.0f || p.J == 0.0f)
 		return fabs(p.v_radial);
-	const double vt = static_cast<double>(p.J) / r;
-	return sqrt(p.v_radial * p.v_radial + vt * vt);
+	const float vt = p.J / r;
+	return static_cast<double>(sqrtf(vr * vr + vt * vt));
+}
+
+// Capture_Energy_eV (src/Simulation_Trajectory.cpp:682-687) in FP32 for the per-step commit
+// (free-flight drift and the uncaptured-bound check); the energy that decides capture and
+// unbinding at a scattering stays FP64.
+__device__ __forceinline__ double capture_energy_eV_f(const DevSolar& S, const DevSolarF& F, double m_dm, float r, float v)
+{
+	float vesc2;
+	if(r > static_cast<float>(DMS_RSUN_KM))
+		vesc2 = static_cast<float>(2.0 * DMS_GMSUN_KM3S2) / r;
+	else
+	{
+		const float rr = r < 0.0f ? 0.0f : r;
+		const int i = knot_index_f(S, F, rr);
+		vesc2 = __ldg(F.vesc2 + i) + (rr - __ldg(F.r + i)) * __ldg(F.vesc2_s + i);
+	}
+	const float scale = static_cast<float>(0.5 * m_dm / (DMS_C_KMS * DMS_C_KMS) / 1.0e-9);
+	return static_cast<double>(scale * (v * v - vesc2));
 }
 
 // Event_In_3D (src/Simulation_Trajectory.cpp:1715-1742) with the angle reduced in FP64 first
@@ -300,6 +321,12 @@ __device__ __forceinline__ float radius_at_fraction_f(const EventF& a, const Eve
 __device__ __forceinline__ bool interior_interval_f(const EventF& a, const EventF& b, double ra, double rb, float& start, float& end)
 {
 	const bool a_in = ra < DMS_RSUN_KM, b_in = rb < DMS_RSUN_KM;
+	if(a_in && b_in)
+	{
+		start = 0.0f;
+		end = 1.0f;
+		return true;
+	}
 	const float dx = b.x.x - a.x.x, dy = b.x.y - a.x.y, dz = b.x.z - a.x.z;
 	const double qa = static_cast<double>(dx * dx + dy * dy + dz * dz);
 	const double qb = 2.0 * static_cast<double>(a.x.x * dx + a.x.y * dy + a.x.z * dz);
@@ -344,12 +371,6 @@ __device__ __forceinline__ bool interior_interval_f(const EventF& a, const Event
 		}
 		return clampf(0.5f * (lower + upper));
 	};
-	if(a_in && b_in)
-	{
-		start = 0.0f;
-		end = 1.0f;
-		return true;
-	}
 	if(!a_in && b_in)
 	{
 		start = (has && in_unit_f(c1)) ? clampf(c1) : (has && in_unit_f(c2)) ? clampf(c2) : bisect();

@@ -323,6 +323,34 @@ __device__ __forceinline__ int free_step(const RunParams& R, const DevPoint* __r
 	return PH_STEP;
 }
 
+// Initial_Conditions + Hyperbolic_Kepler_Shift of every work index (src/Data_Generation.cpp:747-761,
+// src/Simulation_Utilities.cpp:123-321), one thread each, ahead of the trajectory launch: the
+// rejection loops of the halo sampler and the hyperbolic shift run here at full occupancy
+// instead of inside the persistent kernel, where one starting lane would hold its warp.
+__global__ void __launch_bounds__(128) initial_state_kernel(const RunParams R)
+{
+	const uint64_t w = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+	if(w >= R.total)
+		return;
+	const int k = find_range(R, w);
+	const int point = R.range_point[k];
+	Draws D;
+	D.seed = R.seed;
+	D.point = static_cast<uint32_t>(point);
+	D.traj = R.range_first[k] + (w - R.range_offset[k]);
+	D.index = 0;
+	Event ic;
+	const bool ok = initial_conditions(R.S, R.points + point, D, ic, R.ic_max_attempts);
+	if(!ok)
+		atomicOr(R.status, STATUS_IC_REJECTION);
+	const bool shifted = ok && hyperbolic_kepler_shift(ic, R.boundary);
+	InitState st;
+	st.ic = ic;
+	st.draws = static_cast<uint32_t>(D.index);
+	st.flags = (ok ? INIT_IC_OK : 0u) | (shifted ? INIT_SHIFT_OK : 0u);
+	R.init[w] = st;
+}
+
 struct StrictStep
 {
 	__device__ __forceinline__ int operator()(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L, double2* hist) const
@@ -331,7 +359,7 @@ struct StrictStep
 	}
 };
 
-__global__ void __launch_bounds__(128) trajectory_kernel(const RunParams R)
+__global__ void __launch_bounds__(128, DMS_TRAJ_MIN_BLOCKS) trajectory_kernel(const RunParams R)
 {
 	lane_loop<StrictLane>(R, StrictStep());
 }
@@ -402,6 +430,13 @@ double Measure_FP64_Peak(int sm_count, cudaStream_t stream)
 		return -1.0;
 	const double flops = 2.0 * 8.0 * iters * static_cast<double>(blocks) * threads;
 	return flops / (ms * 1.0e-3) / 1.0e12;
+}
+
+void Launch_Initial_States(const RunParams& p, cudaStream_t stream)
+{
+	const uint64_t blocks = (p.total + 127) / 128;
+	if(blocks > 0)
+		initial_state_kernel<<<static_cast<unsigned int>(blocks), 128, 0, stream>>>(p);
 }
 
 void Launch_Trajectories(const RunParams& p, int blocks, int threads, cudaStream_t stream)

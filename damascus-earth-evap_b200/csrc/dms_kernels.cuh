@@ -5,6 +5,15 @@
 
 #include "dms_device.cuh"
 
+// Minimum resident 128-thread blocks per SM the trajectory kernels are compiled for (caps
+// their registers at 65536 / (128 * n)).
+#ifndef DMS_TRAJ_MIN_BLOCKS
+#define DMS_TRAJ_MIN_BLOCKS 4
+#endif
+#ifndef DMS_TRAJ_MIN_BLOCKS_MIXED
+#define DMS_TRAJ_MIN_BLOCKS_MIXED 4
+#endif
+
 namespace dms
 {
 
@@ -17,6 +26,22 @@ enum : unsigned int
 	STATUS_BAD_RANGE = 8u,
 };
 
+// Initial state of one work item, computed for the whole launch before the persistent kernel
+// starts: the event after Initial_Conditions and the Kepler shift to the boundary (the raw
+// initial event when the shift fails), and the uniform draws consumed.
+enum : uint32_t
+{
+	INIT_IC_OK = 1u,     // initial conditions found within the attempt bound
+	INIT_SHIFT_OK = 2u,  // Hyperbolic_Kepler_Shift succeeded
+};
+struct InitState
+{
+	Event ic;
+	uint32_t draws;
+	uint32_t flags;
+};
+static_assert(sizeof(InitState) == 64, "one initial state per 64 bytes");
+
 struct RunParams
 {
 	DevSolar S;
@@ -24,6 +49,8 @@ struct RunParams
 	const float* sf_r;
 	const float* sf_gm;
 	const float* sf_gm_s;
+	const float* sf_vesc2;
+	const float* sf_vesc2_s;
 	const DevPoint* points;
 	int n_points;
 	// work: ranges and their prefix offsets (n_ranges + 1)
@@ -53,10 +80,30 @@ struct RunParams
 	double* rec_hist_v2dt;
 	// per-lane histogram scratch: lanes x DMS_NUM_BINS of (dt, v2dt)
 	double2* lane_hist;
+	// initial state of every work index (written by initial_state_kernel)
+	InitState* init;
 	const volatile int* cancel;
 	unsigned int* status;
 };
 
+// Range of work index w: the largest k with range_offset[k] <= w (binary search).
+__device__ __forceinline__ int find_range(const RunParams& R, uint64_t w)
+{
+	int lo = 0, hi = R.n_ranges - 1;
+	while(lo < hi)
+	{
+		const int mid = (lo + hi + 1) >> 1;
+		if(R.range_offset[mid] <= w)
+			lo = mid;
+		else
+			hi = mid - 1;
+	}
+	return lo;
+}
+
+// Initial states of all p.total work indices into p.init (one thread per work index); the
+// trajectory kernels read them.  Launched on the same stream before every trajectory launch.
+void Launch_Initial_States(const RunParams& p, cudaStream_t stream);
 void Launch_Trajectories(const RunParams& p, int blocks, int threads, cudaStream_t stream);
 void Launch_Rate_Grid(const DevSolar& S, const DevPoint* point, double* grid, int n, cudaStream_t stream);
 void Launch_Rate_Query(const DevSolar& S, const DevPoint* point, int interpolated, const double* r, const double* v, double* out,

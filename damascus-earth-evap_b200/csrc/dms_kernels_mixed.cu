@@ -19,10 +19,12 @@ using MixedLane = LaneT<PropF, EventF>;
 
 // commit_accepted_event (src/Simulation_Trajectory.cpp:842-874) for an FP32 event: bincount
 // with FP64 times, capture energy in FP64.  Returns the energy when evaluated, NaN otherwise.
-__device__ __forceinline__ double commit_event_mixed(const DevSolar& S, double m_dm, int capture_mode, MixedLane& L, double2* hist, const EventF& local)
+__device__ __forceinline__ double commit_event_mixed(const DevSolar& S, const DevSolarF& F, double m_dm, int capture_mode, MixedLane& L, double2* hist,
+                                                     const EventF& local)
 {
-	const double r_now = static_cast<double>(normf(local.x));
-	const double v_now = static_cast<double>(normf(local.v));
+	const float rf = normf(local.x), vf = normf(local.v);
+	const double r_now = static_cast<double>(rf);
+	const double v_now = static_cast<double>(vf);
 	if(!capture_mode)
 	{
 		if(L.prev_time >= 0.0)
@@ -34,7 +36,7 @@ __device__ __forceinline__ double commit_event_mixed(const DevSolar& S, double m
 	const double t_abs = local.t + L.origin;
 	if(capture_mode && !L.is_captured)
 		return NAN;
-	const double E = capture_energy_eV(S, m_dm, r_now, v_now);
+	const double E = capture_energy_eV_f(S, F, m_dm, rf, vf);
 	if(L.is_captured && isfinite(L.free_flight_E))
 	{
 		const double drift = fabs(E - L.free_flight_E);
@@ -60,6 +62,7 @@ __device__ __forceinline__ double commit_event_mixed(const DevSolar& S, double m
 __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, MixedLane& L, double2* hist)
 {
 	const DevSolar& S = R.S;
+	const DevSolarF F{R.sf_r, R.sf_gm, R.sf_gm_s, R.sf_vesc2, R.sf_vesc2_s};
 	const float* grid = reinterpret_cast<const float*>(__ldg(reinterpret_cast<const unsigned long long*>(&P->grid_f)));
 	const int capture_mode = R.capture_mode;
 	const double tau_limit = capture_mode ? DMS_CAPTURE_MAX_OPTICAL_DEPTH_STEP : DMS_MAX_OPTICAL_DEPTH_STEP;
@@ -117,7 +120,6 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 		L.rk_inner = 0;
 	}
 	L.rk_inner++;
-	const DevSolarF F{R.sf_r, R.sf_gm, R.sf_gm_s};
 	const int rk = rk45_attempt_f(S, F, L.pr, L.rk_inner);
 	if(rk == RK_RETRY)
 		return PH_STEP;
@@ -272,7 +274,7 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 				L.seg_steps++;
 				L.steps++;
 				L.retries = 0;
-				commit_event_mixed(S, m_dm, capture_mode, L, hist, boundary_ev);
+				commit_event_mixed(S, F, m_dm, capture_mode, L, hist, boundary_ev);
 				// reset_propagator_at_absolute_event, src/Simulation_Trajectory.cpp:814-822
 				L.cur = inbound;
 				L.cur.t += L.origin;
@@ -290,7 +292,7 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 	L.seg_steps++;
 	L.steps++;
 	L.retries = 0;
-	double E = commit_event_mixed(S, m_dm, capture_mode, L, hist, accepted);
+	double E = commit_event_mixed(S, F, m_dm, capture_mode, L, hist, accepted);
 	L.cur = to_event64(accepted);
 	L.cur.t += L.origin;
 	if(!L.is_captured)
@@ -331,7 +333,7 @@ struct MixedStep
 	}
 };
 
-__global__ void __launch_bounds__(128) trajectory_kernel_mixed(const RunParams R)
+__global__ void __launch_bounds__(128, DMS_TRAJ_MIN_BLOCKS_MIXED) trajectory_kernel_mixed(const RunParams R)
 {
 	lane_loop<MixedLane>(R, MixedStep());
 }

@@ -55,6 +55,9 @@ struct LaneT
 	// bincount anchor (left-endpoint rule)
 	double prev_time, prev_r, prev_v2;
 	int bmin, bmax;
+	// the bin being visited, held in registers until the trajectory leaves it
+	int cbin;
+	double2 cval;
 };
 template <class Lane>
 __device__ __forceinline__ void accumulate_bincount(Lane& L, double2* hist, double r, double v2, double dt)
@@ -71,13 +74,29 @@ __device__ __forceinline__ void accumulate_bincount(Lane& L, double2* hist, doub
 	}
 	if(bin >= 0)
 	{
-		double2 h = hist[bin];
-		h.x += dt;
-		h.y += v2 * dt;
-		hist[bin] = h;
-		L.bmin = bin < L.bmin ? bin : L.bmin;
-		L.bmax = bin > L.bmax ? bin : L.bmax;
+		// The row is read only when a visited bin is entered again and written when it is
+		// left; the additions are the reference's, in its order.
+		if(bin != L.cbin)
+		{
+			if(L.cbin >= 0)
+				hist[L.cbin] = L.cval;
+			L.cval = (bin >= L.bmin && bin <= L.bmax) ? hist[bin] : make_double2(0.0, 0.0);
+			L.cbin = bin;
+			L.bmin = bin < L.bmin ? bin : L.bmin;
+			L.bmax = bin > L.bmax ? bin : L.bmax;
+		}
+		L.cval.x += dt;
+		L.cval.y += v2 * dt;
 	}
+}
+
+// Writes the bin being visited back to the lane's row (before the row is read out).
+template <class Lane>
+__device__ __forceinline__ void write_back_bin(Lane& L, double2* hist)
+{
+	if(L.cbin >= 0)
+		hist[L.cbin] = L.cval;
+	L.cbin = -1;
 }
 
 // Update_Capture_State, src/Simulation_Trajectory.cpp:689-760
@@ -195,8 +214,22 @@ __device__ __forceinline__ bool is_computational_truncation(int r)
 
 // Termination: tail of Simulate (src/Simulation_Trajectory.cpp:1349-1399), classification and
 // aggregation of simulate_one_trajectory (src/Data_Generation.cpp:745-861).
+// The lane's histogram row still to be moved out at termination: copied into the record's
+// histograms (records mode) or added with its squares to the per-point sums (accumulate mode),
+// and zeroed either way.  Executed by the whole warp (cooperative_flush).
+struct FlushJob
+{
+	double* dst0;  // records: dt row; accumulate: sum of dt
+	double* dst1;  // records: v2dt row; accumulate: sum of v2dt
+	double* dst2;  // accumulate: sum of dt^2
+	double* dst3;  // accumulate: sum of v2dt^2
+	int b0, b1;    // touched bins; b1 < b0 when there is nothing to do
+	int mode;      // FLUSH_ZERO, FLUSH_COPY or FLUSH_ADD
+};
+constexpr int FLUSH_ZERO = 0, FLUSH_COPY = 1, FLUSH_ADD = 2;
+
 template <class Lane>
-__device__ __noinline__ void finalize(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, Lane& L, double2* hist)
+__device__ __noinline__ void finalize(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, Lane& L, FlushJob& job)
 {
 	const DevSolar& S = R.S;
 	int reason = L.reason;
@@ -280,7 +313,9 @@ __device__ __noinline__ void finalize(const RunParams& R, const DevPoint* __rest
 	const double life = observed ? L.t_final_unbinding - L.t_capture : -1.0;
 	const double lifetime = (L.is_captured && isfinite(life) && life >= 0.0) ? life : -1.0;
 
-	const int b0 = L.bmin, b1 = L.bmax;
+	job.b0 = L.bmin;
+	job.b1 = L.bmax;
+	job.mode = FLUSH_ZERO;
 	if(R.records != nullptr)
 	{
 		dms_traj_record& rec = R.records[L.work - 0];
@@ -305,14 +340,9 @@ __device__ __noinline__ void finalize(const RunParams& R, const DevPoint* __rest
 		rec.lifetime_unbinding = lifetime;
 		if(R.rec_hist_dt != nullptr)
 		{
-			double* hd = R.rec_hist_dt + L.work * DMS_NUM_BINS;
-			double* hv = R.rec_hist_v2dt + L.work * DMS_NUM_BINS;
-			for(int b = b0; b <= b1; b++)
-			{
-				const double2 h = hist[b];
-				hd[b] = h.x;
-				hv[b] = h.y;
-			}
+			job.mode = FLUSH_COPY;
+			job.dst0 = R.rec_hist_dt + L.work * DMS_NUM_BINS;
+			job.dst1 = R.rec_hist_v2dt + L.work * DMS_NUM_BINS;
 		}
 	}
 	else
@@ -377,33 +407,70 @@ __device__ __noinline__ void finalize(const RunParams& R, const DevPoint* __rest
 		if(hist_slot >= 0)
 		{
 			double* h = R.hists + static_cast<size_t>(L.point) * DMS_NUM_HISTS * DMS_NUM_BINS;
-			double* h_dt = h + (hist_slot + 0) * DMS_NUM_BINS;
-			double* h_v2 = h + (hist_slot + 1) * DMS_NUM_BINS;
-			double* h_dt_sq = h + (hist_slot + 4) * DMS_NUM_BINS;
-			double* h_v2_sq = h + (hist_slot + 5) * DMS_NUM_BINS;
-			for(int b = b0; b <= b1; b++)
-			{
-				const double2 x = hist[b];
-				if(x.x != 0.0 || x.y != 0.0)
-				{
-					atomicAdd(h_dt + b, x.x);
-					atomicAdd(h_v2 + b, x.y);
-					atomicAdd(h_dt_sq + b, x.x * x.x);
-					atomicAdd(h_v2_sq + b, x.y * x.y);
-				}
-			}
+			job.mode = FLUSH_ADD;
+			job.dst0 = h + (hist_slot + 0) * DMS_NUM_BINS;
+			job.dst1 = h + (hist_slot + 1) * DMS_NUM_BINS;
+			job.dst2 = h + (hist_slot + 4) * DMS_NUM_BINS;
+			job.dst3 = h + (hist_slot + 5) * DMS_NUM_BINS;
 		}
 	}
-	for(int b = b0; b <= b1; b++) hist[b] = make_double2(0.0, 0.0);
 }
 
-// Picks up work index `w`: trajectory start = Initial_Conditions + Hyperbolic_Kepler_Shift and the
-// Simulate prologue (src/Data_Generation.cpp:747-761, src/Simulation_Trajectory.cpp:1284-1308).
+// Moves the histogram rows of every lane of the converged group that terminated in this
+// iteration: all lanes of the group stride over one row at a time, so the row is read, the
+// per-point sums are updated and the row is zeroed with coalesced accesses instead of one
+// lane walking up to 2000 bins while the rest of its warp waits.
+__device__ __forceinline__ void cooperative_flush(double2* hist, FlushJob& job)
+{
+	const unsigned int grp = __activemask();
+	unsigned int pending = __ballot_sync(grp, job.b1 >= job.b0);
+	if(pending == 0u)
+		return;
+	const int me = threadIdx.x & 31;
+	const int rank = __popc(grp & ((1u << me) - 1u));
+	const int size = __popc(grp);
+	__syncwarp(grp);  // each owner's last write to its row is visible to the group
+	while(pending != 0u)
+	{
+		const int leader = __ffs(pending) - 1;
+		pending &= pending - 1u;
+		double2* row = reinterpret_cast<double2*>(__shfl_sync(grp, reinterpret_cast<unsigned long long>(hist), leader));
+		const int b0 = __shfl_sync(grp, job.b0, leader);
+		const int b1 = __shfl_sync(grp, job.b1, leader);
+		const int mode = __shfl_sync(grp, job.mode, leader);
+		double* d0 = reinterpret_cast<double*>(__shfl_sync(grp, reinterpret_cast<unsigned long long>(job.dst0), leader));
+		double* d1 = reinterpret_cast<double*>(__shfl_sync(grp, reinterpret_cast<unsigned long long>(job.dst1), leader));
+		double* d2 = reinterpret_cast<double*>(__shfl_sync(grp, reinterpret_cast<unsigned long long>(job.dst2), leader));
+		double* d3 = reinterpret_cast<double*>(__shfl_sync(grp, reinterpret_cast<unsigned long long>(job.dst3), leader));
+		for(int b = b0 + rank; b <= b1; b += size)
+		{
+			const double2 x = row[b];
+			if(mode == FLUSH_COPY)
+			{
+				d0[b] = x.x;
+				d1[b] = x.y;
+			}
+			else if(mode == FLUSH_ADD && (x.x != 0.0 || x.y != 0.0))
+			{
+				atomicAdd(d0 + b, x.x);
+				atomicAdd(d1 + b, x.y);
+				atomicAdd(d2 + b, x.x * x.x);
+				atomicAdd(d3 + b, x.y * x.y);
+			}
+			row[b] = make_double2(0.0, 0.0);
+		}
+	}
+	__syncwarp(grp);  // the zeroed rows are visible to their owners before they are reused
+	job.b1 = -1;
+}
+
+// Picks up work index `w`: the Simulate prologue (src/Simulation_Trajectory.cpp:1284-1308) from
+// the initial state (Initial_Conditions + Hyperbolic_Kepler_Shift, src/Data_Generation.cpp:747-761)
+// that initial_state_kernel computed for every work index before the launch.
 template <class Lane>
 __device__ __forceinline__ int start_trajectory(const RunParams& R, Lane& L, uint64_t w, const DevPoint*& P, double& m_dm)
 {
-	int k = 0;
-	while(k + 1 < R.n_ranges && w >= R.range_offset[k + 1]) k++;
+	const int k = find_range(R, w);
 	L.work = w;
 	L.point = R.range_point[k];
 	P = R.points + L.point;
@@ -428,12 +495,12 @@ __device__ __forceinline__ int start_trajectory(const RunParams& R, Lane& L, uin
 	L.prev_v2 = 0.0;
 	L.bmin = DMS_NUM_BINS;
 	L.bmax = -1;
+	L.cbin = -1;
 	L.reason = DMS_REASON_UNKNOWN;
-	Event ic;
-	const bool ic_ok = initial_conditions(R.S, P, L.D, ic, R.ic_max_attempts);
-	if(!ic_ok)
-		atomicOr(R.status, STATUS_IC_REJECTION);
-	L.shift_ok = ic_ok && hyperbolic_kepler_shift(ic, R.boundary);
+	const InitState& init = R.init[w];
+	const Event ic = init.ic;
+	L.D.index = init.draws;
+	L.shift_ok = (init.flags & INIT_SHIFT_OK) != 0u;
 	L.cur = ic;
 	if(R.records != nullptr)
 	{
@@ -535,6 +602,9 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	__shared__ double coop_rates[4][DMS_NUM_TARGETS + 1];  // blocks of at most 128 threads
 	double* rates = coop_rates[threadIdx.x >> 5];
 	Lane L;
+	FlushJob job;
+	job.b0 = 0;
+	job.b1 = -1;
 	const DevPoint* P = R.points;
 	double m_dm = 0.0;
 	int phase = PH_FETCH;
@@ -579,9 +649,11 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 			phase = finish_scatter(R, P, m_dm, L, target);
 		if(phase == PH_FINAL)
 		{
-			finalize(R, P, m_dm, L, hist);
+			write_back_bin(L, hist);
+			finalize(R, P, m_dm, L, job);
 			phase = PH_FETCH;
 		}
+		cooperative_flush(hist, job);
 	}
 	if(phase != PH_FETCH && L.bmax >= L.bmin)
 		for(int b = L.bmin; b <= L.bmax; b++) hist[b] = make_double2(0.0, 0.0);

@@ -45,6 +45,64 @@ def binned_means(res, slot=HIST_CAPTURED_DT, slot_sq=HIST_CAPTURED_DT_SQ):
     return mean, var_sum / (n * n)
 
 
+def wilson_interval(successes, trials, z=1.959963984540054):
+    """95 % Wilson score interval of a binomial rate."""
+    if trials <= 0:
+        return 0.0, 0.0
+    p = successes / trials
+    den = 1.0 + z * z / trials
+    centre = (p + z * z / (2.0 * trials)) / den
+    half = z * math.sqrt(p * (1.0 - p) / trials + z * z / (4.0 * trials * trials)) / den
+    return centre - half, centre + half
+
+
+def _quantile(values, q):
+    v = np.sort(np.asarray(values, dtype=np.float64))
+    if len(v) == 0:
+        return None
+    x = q * (len(v) - 1)
+    lo, hi = int(math.floor(x)), int(math.ceil(x))
+    return float(v[lo] + (x - lo) * (v[hi] - v[lo]))
+
+
+def reference_gates(ref, other, min_events=30):
+    """The reference's ensemble acceptance checks (validation/physics_validation.py:192-309),
+    restated on engine results: 95 % capture intervals overlap, complete-evaporation fraction
+    z <= 3, mean scatterings within 10 %, captured radial distribution total variation <= 0.10,
+    evaporation-time median within 20 % and 90th percentile within 30 % (when both runs have
+    at least `min_events` events).  Returns {name: (passed, value)}."""
+    ca, cb = ref["counters"], other["counters"]
+    out = {}
+    ia = wilson_interval(ca["captured"], ca["trajectories"])
+    ib = wilson_interval(cb["captured"], cb["trajectories"])
+    out["capture_95pct_intervals_overlap"] = (max(ia[0], ib[0]) <= min(ia[1], ib[1]), [ia, ib])
+    ea, eb = len(ref["events"]), len(other["events"])
+    na, nb = ca["captured"], cb["captured"]
+    if na > 0 and nb > 0:
+        pooled = (ea + eb) / (na + nb)
+        var = pooled * (1.0 - pooled) * (1.0 / na + 1.0 / nb)
+        diff = abs(ea / na - eb / nb)
+        z = (0.0 if diff == 0.0 else math.inf) if var <= 0.0 else diff / math.sqrt(var)
+        out["complete_evaporation_fraction_z"] = (z <= 3.0, z)
+    sa = ca["total_scatterings"] / max(ca["trajectories"], 1)
+    sb = cb["total_scatterings"] / max(cb["trajectories"], 1)
+    d = abs(sb - sa) / max(abs(sa), 1.0)
+    out["average_scatterings_relative_difference"] = (d <= 0.10, d)
+    ha = np.asarray(ref["histograms"][HIST_CAPTURED_DT], dtype=np.float64)
+    hb = np.asarray(other["histograms"][HIST_CAPTURED_DT], dtype=np.float64)
+    if ha.sum() > 0 and hb.sum() > 0:
+        tv = 0.5 * float(np.sum(np.abs(hb / hb.sum() - ha / ha.sum())))
+        out["captured_radial_total_variation"] = (tv <= 0.10, tv)
+    if ea >= min_events and eb >= min_events:
+        la, lb = ref["events"]["lifetime_unbinding"], other["events"]["lifetime_unbinding"]
+        for name, q, limit in (("evaporation_median_relative_difference", 0.5, 0.20),
+                               ("evaporation_p90_relative_difference", 0.9, 0.30)):
+            qa, qb = _quantile(la, q), _quantile(lb, q)
+            d = abs(qb - qa) / max(abs(qa), 1.0e-300)
+            out[name] = (d <= limit, d)
+    return out
+
+
 def compare_runs(ref, other):
     """Error of `other` against `ref` (both Engine.results() dictionaries of the same point)."""
     ca, cb = ref["counters"], other["counters"]

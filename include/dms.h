@@ -201,15 +201,16 @@ int dms_run_records(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64
  * memory when it runs: it allocates nothing.  d_records (count records) and, when non-null,
  * d_hist_dt / d_hist_v2dt (count * 2000 doubles each) are DEVICE buffers owned by the caller,
  * filled with the same values dms_run_records returns.  The run's scratch (work queue, status
- * word, one 2000-bin histogram row per lane) is a fixed array of DMS_NOALLOC_SCRATCH_BYTES in
- * the library's device image, so at most DMS_NOALLOC_MAX_TRAJECTORIES trajectories fit one
+ * word, initial states, one 2000-bin histogram row per lane) is a fixed array of
+ * DMS_NOALLOC_SCRATCH_BYTES in the library's device image, so at most
+ * DMS_NOALLOC_MAX_TRAJECTORIES trajectories fit one
  * call; larger counts return DMS_ERR_INVALID_ARGUMENT.  The FP64 kernel runs whatever
  * opts->precision says, with one lane per trajectory (threads_per_block and blocks_per_sm are
  * ignored).  The first call on a device looks the array up; make that call before any stream
  * capture on that device starts.  Every call on a device shares the array: calls that overlap
  * on the GPU (two contexts or two host threads on one device) race. */
 #define DMS_NOALLOC_MAX_TRAJECTORIES 128
-#define DMS_NOALLOC_SCRATCH_BYTES    (256 + DMS_NOALLOC_MAX_TRAJECTORIES * 2000 * 16)
+#define DMS_NOALLOC_SCRATCH_BYTES    (256 + DMS_NOALLOC_MAX_TRAJECTORIES * (64 + 2000 * 16))
 int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64_t first, uint64_t count,
                             dms_traj_record* d_records, double* d_hist_dt, double* d_hist_v2dt);
 

@@ -41,3 +41,23 @@ def test_capture_fraction_sigmas():
     sigma = np.sqrt(0.05 * 0.95 / 10000 + 0.056 * 0.944 / 10000)
     assert abs(c["capture_fraction_sigmas"] - 0.006 / sigma) < 1e-9
     assert abs(c["capture_fraction_rel_error"] - 0.12) < 1e-12
+
+
+def test_reference_gates_pass_for_same_distribution_and_fail_for_shift():
+    a = fake_results(100000, 5000, 2.0, 2000, seed=1)
+    rng = np.random.default_rng(5)
+    a["events"]["lifetime_unbinding"] = rng.exponential(1e6, 2000)
+    b = fake_results(100000, 5040, 2.0, 2010, seed=2)
+    b["events"]["lifetime_unbinding"] = rng.exponential(1e6, 2010)
+    g = dms_stats.reference_gates(a, b)
+    assert all(ok for ok, _ in g.values()), g
+    c = fake_results(100000, 8000, 2.0, 2000, seed=2)
+    c["counters"]["total_scatterings"] = 13 * 100000
+    g = dms_stats.reference_gates(a, c)
+    assert not g["capture_95pct_intervals_overlap"][0]
+    assert not g["average_scatterings_relative_difference"][0]
+
+
+def test_wilson_interval_contains_rate():
+    lo, hi = dms_stats.wilson_interval(50, 1000)
+    assert lo < 0.05 < hi and abs((hi - lo) - 0.0276) < 2e-3
