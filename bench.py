@@ -45,6 +45,10 @@ WORKLOAD = ("Parameter-point evaporation (config 1): SI contact m=0.3 GeV sigma_
 # (64-channel rate sum, free-gas target velocity, kinematics) and per trajectory (initial
 # conditions, Kepler shift, classification).
 FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ = 214.8, 622.3, 2455.0, 3374.0
+# DRAM bytes (read + write) of the FP64 trajectory kernel per trajectory of this point, from one
+# ncu capture of 2^19 trajectories (73 GB); almost all of it is the termination flush of the
+# per-lane histogram row.
+TRAFFIC_PER_TRAJECTORY = 73.0e9 / (1 << 19)
 
 
 def log(*a):
@@ -220,11 +224,15 @@ def run_engine_arm(args):
     import dms_b200
     import dms_stats
     engine = dms_b200.Engine(local_rank)
-    pid = engine.add_point(dms_b200.point_params(MASS_GEV, SIGMA_CM2, interpolation_points=GRID_N))
-    opts = {prec: dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT, time_limit_s=600.0,
-                                    precision=prec)
-            for prec in (dms_b200.PRECISION_FP64, dms_b200.PRECISION_MIXED)}
+    params = dms_b200.point_params(MASS_GEV, SIGMA_CM2, interpolation_points=GRID_N)
+    K = args.steps
+    # one accumulator slot (a copy of the point) per timed step, so that the K steps of one
+    # launch keep separate results; slot `solo` serves the warm-up, isolated and steady runs
+    pids = [engine.add_point(params) for _ in range(K)]
+    solo = engine.add_point(params)
     fp64, mixed = dms_b200.PRECISION_FP64, dms_b200.PRECISION_MIXED
+    opts = {prec: dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT, time_limit_s=600.0,
+                                    precision=prec) for prec in (fp64, mixed)}
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     peak = engine.fp64_peak_tflops()
 
@@ -236,60 +244,81 @@ def run_engine_arm(args):
     def ids(step):
         return (step * world + rank) * TRAJECTORIES
 
-    def timed_steps(prec, first_step, events_capacity):
-        """K steps of one form: device time of the launches and the summed results."""
+    def batch(first_step):
+        return [(pids[s], ids(first_step + s), TRAJECTORIES) for s in range(K)]
+
+    # warm-up: W isolated steps per form; the last one of each gives the isolated step time
+    isolated = {}
+    for prec in (fp64, mixed):
+        for w in range(args.warmup):
+            engine.reset_results(solo)
+            engine.run([(solo, ids(w), TRAJECTORIES)], opts[prec])
+            isolated[prec] = engine.last_kernel_ms()
+            flush.zero_()
+
+    def timed(prec, first_step):
+        """K steps of one form in one launch: device time and per-step results."""
+        for p in pids:
+            engine.reset_results(p)
         clocks = ClockSampler(local_rank)
         clocks.start()
         barrier()
-        ms = 0.0
-        acc = None
-        min_captured = None
-        for s in range(args.steps):
-            engine.reset_results(pid)
-            engine.run([(pid, ids(first_step + s), TRAJECTORIES)], opts[prec])
-            ms += engine.last_kernel_ms()
-            res = engine.results(pid, events_capacity=events_capacity)
-            acc = add_results(acc, res)
-            c = res["counters"]["captured"]
-            min_captured = c if min_captured is None else min(min_captured, c)
-            flush.zero_()
+        engine.run(batch(first_step), opts[prec])
         barrier()
-        return ms, acc, min_captured, clocks.stop()
+        ms = engine.last_kernel_ms()
+        info = clocks.stop()
+        per_step = [engine.results(p, events_capacity=1 << 16) for p in pids]
+        acc = None
+        for r in per_step:
+            acc = add_results(acc, r)
+        return ms, acc, min(r["counters"]["captured"] for r in per_step), info
 
-    # warm-up (both forms)
-    for w in range(args.warmup):
-        for prec in (fp64, mixed):
-            engine.reset_results(pid)
-            engine.run([(pid, ids(w), TRAJECTORIES)], opts[prec])
-            flush.zero_()
-    # timed region: FP64 form (the headline), then the mixed form on the same trajectory ids
-    dev_ms, tot, min_captured, clock_info = timed_steps(fp64, args.warmup, 1 << 16)
-    mix_ms, mix_tot, _, mix_clocks = timed_steps(mixed, args.warmup, 1 << 16) if not args.no_mixed else (0.0, None, 0, None)
-    # e2e: through the C ABI with host buffers; every step copies its work range in and its
-    # counters, histograms and evaporation events out
+    dev_ms, tot, min_captured, clock_info = timed(fp64, args.warmup)
+    flush.zero_()
+    if not args.no_mixed:
+        mix_ms, mix_tot, _, mix_clocks = timed(mixed, args.warmup)
+        flush.zero_()
+    # e2e: the same K steps through the C ABI from the host, fresh ids: work ranges in, then
+    # every step's counters, histograms and evaporation events out
+    for p in pids:
+        engine.reset_results(p)
     barrier()
     t0 = time.perf_counter()
+    engine.run(batch(args.warmup + K), opts[fp64])
     e2e_scat = 0
     d2h_bytes = 0
-    for s in range(args.steps):
-        engine.reset_results(pid)
-        engine.run([(pid, ids(args.warmup + args.steps + s), TRAJECTORIES)], opts[fp64])
-        res = engine.results(pid, events_capacity=1 << 16)
+    for p in pids:
+        res = engine.results(p, events_capacity=1 << 16)
         e2e_scat += res["counters"]["total_scatterings"]
         d2h_bytes += 8 * 32 + res["histograms"].nbytes + 16 * len(res["events"])
     barrier()
     e2e_s = time.perf_counter() - t0
+    # steady state: a queue far longer than the run, stopped by the wall-clock limit; every
+    # scattering done counts, in finished and in unfinished trajectories
+    steady = {}
+    if args.steady_seconds > 0:
+        for name, prec in (("fp64", fp64), ("mixed", mixed)):
+            engine.reset_results(solo)
+            o = dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT,
+                                  time_limit_s=args.steady_seconds, precision=prec)
+            try:
+                engine.run([(solo, 1 << 40, 1 << 21)], o)
+            except dms_b200.EngineError as e:
+                if "cancelled" not in str(e):
+                    raise
+            ms = engine.last_kernel_ms()
+            c = engine.results(solo, events_capacity=1)["counters"]
+            steady[name] = {"scatterings_per_s": (c["total_scatterings"] + c["unfinished_scatterings"]) / ms * 1e3,
+                            "steps_per_s": (c["rk_steps"] + c["unfinished_rk_steps"]) / ms * 1e3,
+                            "kernel_ms": ms}
+        steady["mixed_over_fp64"] = steady["mixed"]["scatterings_per_s"] / steady["fp64"]["scatterings_per_s"]
 
     c = tot["counters"]
     totals = torch.tensor([float(c["total_scatterings"]), float(c["trajectories"]), float(e2e_scat)],
                           dtype=torch.float64, device="cuda")
-    times = torch.tensor([dev_ms, e2e_s, mix_ms], dtype=torch.float64, device="cuda")
-    mix_totals = torch.tensor([float(mix_tot["counters"]["total_scatterings"]) if mix_tot else 0.0,
-                               float(mix_tot["counters"]["trajectories"]) if mix_tot else 0.0],
-                              dtype=torch.float64, device="cuda")
+    times = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(totals, op=dist.ReduceOp.SUM)
-        dist.all_reduce(mix_totals, op=dist.ReduceOp.SUM)
         dist.all_reduce(times, op=dist.ReduceOp.MAX)
     dev_s = float(times[0]) * 1e-3
     value = float(totals[0]) / dev_s
@@ -301,39 +330,51 @@ def run_engine_arm(args):
     line = None
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "scatterings/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "metric": METRIC, "value": value, "unit": "scatterings/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": dev_ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "trajectories_per_s": traj_rate,
             "captured_per_step_min": min_captured,
+            "isolated_step_ms": {"fp64": isolated[fp64], "mixed": isolated[mixed]},
             "config": {"workload": WORKLOAD, "mass_gev": MASS_GEV, "sigma_cm2": SIGMA_CM2, "grid": GRID_N,
                        "trajectories_per_gpu_step": TRAJECTORIES, "seed": SEED, "precision": "fp64 (no FMA contraction)",
+                       "steps_submission": "the K timed steps are K batches (one accumulator slot each) of one "
+                                           "persistent launch, so they share one tail; isolated_step_ms is one "
+                                           "batch launched alone",
                        "parallelism": "trajectory ids sharded over %d GPU(s), no data-path collective" % world,
-                       "l2": "per-lane histogram scratch > L2, plus 256 MB flush between steps"},
-            "e2e": {"value": e2e_value, "unit": "scatterings/s", "h2d_bytes_per_step": 64,
-                    "d2h_bytes_per_step": int(d2h_bytes / max(args.steps, 1))},
-            "gpu_launches": args.steps,
+                       "l2": "per-lane histogram scratch (2.4 GB) exceeds L2; 256 MB flush between launches"},
+            "e2e": {"value": e2e_value, "unit": "scatterings/s", "h2d_bytes_per_step": 24,
+                    "d2h_bytes_per_step": int(d2h_bytes / max(K, 1))},
+            "gpu_launches": 2,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                         "frac": achieved / peak if peak > 0 else None,
+                         "traffic": TRAFFIC_PER_TRAJECTORY * c["trajectories"],
+                         "traffic_source": "ncu dram__bytes of a 2^19-trajectory launch of this point, per trajectory x "
+                                           "trajectories of this launch",
                          "peak_source": "measured in this run: DFMA-chain kernel on all SMs (2 FLOP per FMA)",
                          "flop_model": "%.1f/attempt + %.1f/step + %.0f/scattering + %.0f/trajectory (counted)" % (
                              FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ)},
             "clocks": clock_info,
         }
-        if mix_tot is not None:
-            mix_s = float(times[2]) * 1e-3
+        if steady:
+            line["steady_state"] = steady
+        if not args.no_mixed:
+            mix_s = mix_ms * 1e-3
+            mc = mix_tot["counters"]
             err = dms_stats.compare_runs(tot, mix_tot)
+            gates = dms_stats.reference_gates(tot, mix_tot)
             line["mixed"] = {
-                "value": float(mix_totals[0]) / mix_s, "unit": "scatterings/s",
-                "trajectories_per_s": float(mix_totals[1]) / mix_s, "ms_per_step": float(times[2]) / args.steps,
-                "speedup_vs_fp64": (float(mix_totals[0]) / mix_s) / value,
-                "dtype": "f32 stages/geometry/rates + f64 state, energy, error norm, optical depth, accumulators",
+                "value": mc["total_scatterings"] / mix_s, "unit": "scatterings/s",
+                "trajectories_per_s": mc["trajectories"] / mix_s, "ms_per_step": mix_ms / K,
+                "speedup_vs_fp64": (mc["total_scatterings"] / mix_s) / (c["total_scatterings"] / (dev_ms * 1e-3)),
+                "dtype": "f32 stages/geometry/rates + f64 state, energy at scatterings, error norm, optical depth, accumulators",
                 "error_vs_fp64": {k: err[k] for k in ("capture_fraction_rel_error", "capture_fraction_sigmas",
                                                       "radial_chi2", "radial_dof", "radial_p_value",
                                                       "radial_max_bin_deviation", "evaporation_rate_rel_error",
                                                       "mean_scatterings_rel_error")},
+                "reference_gates": {k: {"pass": bool(ok), "value": v} for k, (ok, v) in gates.items()},
                 "clocks": mix_clocks,
-                "gpu_launches": args.steps,
+                "gpu_launches": 2,
             }
     engine.close()
     if world > 1:
@@ -348,25 +389,82 @@ def run_engine_arm(args):
                                     "kind": cpu_kind(),
                                     "sample": "%d trajectories of the same point, %.0f s on every core" % (
                                         ntraj, args.cpu_baseline_seconds)}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, default=float), flush=True)
+
+
+GRID_MASSES = (0.1, 0.3, 1.0, 3.0)
+GRID_SIGMAS = (1e-39, 1e-38, 1e-37, 1e-36, 1e-35)
+GRID_PER_POINT = 1 << 17
+GRID_MAX_SCAT = 10 ** 5
+
+
+def run_grid(args):
+    """The 20-point mass x cross-section grid in one persistent launch per form (2^17
+    trajectories per point, 2^21 in all, max 1e5 scatterings).  Its heavy points (m >= 1 GeV at
+    sigma >= 1e-37 cm^2) capture particles that scatter up to the cap, so the full launch is
+    hours of work; it runs for a bounded wall time and the rate counts every scattering done,
+    in finished trajectories and in those the time limit left unfinished."""
+    import dms_b200
+    engine = dms_b200.Engine(0)
+    pids = [engine.add_point(dms_b200.point_params(m, s, interpolation_points=GRID_N))
+            for m in GRID_MASSES for s in GRID_SIGMAS]
+    out = {"workload": "20-point grid m in %s GeV x sigma_n in %s cm2, %d trajectories per point, max %d scatterings, "
+                       "seed %d, bounded to %.0f s per form" % (list(GRID_MASSES), list(GRID_SIGMAS), GRID_PER_POINT,
+                                                               GRID_MAX_SCAT, SEED, args.grid_seconds)}
+    for name, prec in (("fp64", dms_b200.PRECISION_FP64), ("mixed", dms_b200.PRECISION_MIXED)):
+        for pid in pids:
+            engine.reset_results(pid)
+        opts = dms_b200.run_opts(seed=SEED, max_scatterings=GRID_MAX_SCAT, time_limit_s=args.grid_seconds, precision=prec)
+        try:
+            engine.run([(pid, 0, GRID_PER_POINT) for pid in pids], opts)
+            finished = True
+        except dms_b200.EngineError as e:
+            if "cancelled" not in str(e):
+                raise
+            finished = False
+        ms = engine.last_kernel_ms()
+        tot = {k: 0 for k in ("trajectories", "total_scatterings", "rk_steps", "unfinished_trajectories",
+                              "unfinished_scatterings", "unfinished_rk_steps", "captured")}
+        for pid in pids:
+            c = engine.results(pid, events_capacity=1)["counters"]
+            for k in tot:
+                tot[k] += c[k]
+        scat = tot["total_scatterings"] + tot["unfinished_scatterings"]
+        steps = tot["rk_steps"] + tot["unfinished_rk_steps"]
+        out[name] = {"kernel_ms": ms, "finished": finished, "scatterings_per_s": scat / ms * 1e3,
+                     "steps_per_s": steps / ms * 1e3, "finished_trajectories_per_s": tot["trajectories"] / ms * 1e3,
+                     "counters": tot}
+    out["mixed_over_fp64_scatterings_per_s"] = out["mixed"]["scatterings_per_s"] / out["fp64"]["scatterings_per_s"]
+    print(json.dumps(out), flush=True)
+    engine.close()
 
 
 def run_profile_case(args):
-    """One trajectory launch for a profiler (no timing, no JSON line): `single` runs trajectory
-    id 1612 alone (the longest of ids 0..16383 of this point, 38944 accepted steps in the FP64
-    form: the per-lane latency of the tail), `saturated` runs 2^19 trajectories (about seven per
-    resident lane: the bulk throughput), `step` runs one bench step (65536 trajectories)."""
+    """One trajectory launch for a profiler (no timing): `single` runs trajectory id 1612 alone
+    (the longest of ids 0..16383 of this point, 38944 accepted steps in the FP64 form: the
+    per-lane latency of the tail), `saturated` runs 2^19 trajectories (about seven per resident
+    lane, with the batch's tail), `steady` runs a queue of 2^21 trajectories that every lane
+    leaves after 1024 loop iterations (the steady state without a tail; the stop is the same in
+    every profiler pass), `step` runs one bench step (65536 trajectories)."""
     import dms_b200
     prec = dms_b200.PRECISION_MIXED if args.precision == "mixed" else dms_b200.PRECISION_FP64
     engine = dms_b200.Engine(0)
     pid = engine.add_point(dms_b200.point_params(MASS_GEV, SIGMA_CM2, interpolation_points=GRID_N))
-    opts = dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT, time_limit_s=300.0, precision=prec)
-    first, count = {"single": (1612, 1), "saturated": (0, 1 << 19), "step": (0, TRAJECTORIES)}[args.profile_case]
-    engine.run([(pid, first, count)], opts)
+    budget = 1024 if args.profile_case == "steady" else 0
+    opts = dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT, time_limit_s=300.0, precision=prec,
+                             iteration_budget=budget)
+    first, count = {"single": (1612, 1), "saturated": (0, 1 << 19), "steady": (0, 1 << 21),
+                    "step": (0, TRAJECTORIES)}[args.profile_case]
+    try:
+        engine.run([(pid, first, count)], opts)
+    except dms_b200.EngineError as e:
+        if not budget or "budget" not in str(e):
+            raise
     c = engine.results(pid, events_capacity=1)["counters"]
     print(json.dumps({"profile_case": args.profile_case, "precision": args.precision, "kernel_ms": engine.last_kernel_ms(),
-                      "trajectories": c["trajectories"], "rk_steps": c["rk_steps"], "rk_attempts": c["rk_attempts"],
-                      "scatterings": c["total_scatterings"]}), flush=True)
+                      "trajectories": c["trajectories"], "rk_steps": c["rk_steps"] + c["unfinished_rk_steps"],
+                      "rk_attempts": c["rk_attempts"] + c["unfinished_rk_attempts"],
+                      "scatterings": c["total_scatterings"] + c["unfinished_scatterings"]}), flush=True)
     engine.close()
 
 
@@ -378,13 +476,19 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
+    ap.add_argument("--steady-seconds", type=float, default=2.0,
+                    help="length of the steady-state measurement per form (0 skips it)")
     ap.add_argument("--cpu-baseline-seconds", type=float, default=12.0)
     ap.add_argument("--reference-step-seconds", type=float, default=6.0)
-    ap.add_argument("--profile-case", choices=["single", "saturated", "step"],
+    ap.add_argument("--profile-case", choices=["single", "saturated", "steady", "step"],
                     help="run one trajectory launch for a profiler and exit")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64", help="form used by --profile-case")
+    ap.add_argument("--grid-seconds", type=float, default=0.0,
+                    help="run the 20-point grid launch for this many seconds per form instead of the bench")
     args = ap.parse_args()
-    if args.profile_case:
+    if args.grid_seconds > 0:
+        run_grid(args)
+    elif args.profile_case:
         run_profile_case(args)
     elif args.impl == "reference":
         run_reference_arm(args)

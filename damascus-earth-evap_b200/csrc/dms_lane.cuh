@@ -3,6 +3,8 @@
 // aggregation.  The free step itself (the Propagate_Freely loop body) is supplied by each form.
 #pragma once
 
+#include <type_traits>
+
 #include "dms_kernels.cuh"
 
 namespace dms
@@ -26,6 +28,9 @@ enum Phase : int
 template <class PropT, class EvT>
 struct LaneT
 {
+	// the FP64 form bins by the reference's division; the mixed form multiplies by the
+	// reciprocal bin width (a bin edge can then move by one ulp)
+	static constexpr bool exact_bins = std::is_same<PropT, Prop>::value;
 	uint64_t work;
 	int point;
 	Draws D;
@@ -68,7 +73,10 @@ __device__ __forceinline__ void accumulate_bincount(Lane& L, double2* hist, doub
 	int bin = -1;
 	if(isfinite(r) && r >= 0.0 && r < DMS_BIN_MAX_KM)
 	{
-		bin = static_cast<int>(r / DMS_BIN_WIDTH_KM);
+		if constexpr(Lane::exact_bins)
+			bin = static_cast<int>(r / DMS_BIN_WIDTH_KM);
+		else
+			bin = static_cast<int>(r * (1.0 / DMS_BIN_WIDTH_KM));
 		if(bin < 0) bin = 0;
 		if(bin >= DMS_NUM_BINS) bin = -1;
 	}
@@ -657,6 +665,15 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	}
 	if(phase != PH_FETCH && L.bmax >= L.bmin)
 		for(int b = L.bmin; b <= L.bmax; b++) hist[b] = make_double2(0.0, 0.0);
+	if(phase != PH_FETCH && R.records == nullptr)
+	{
+		// stopped in mid-trajectory: count the work done so far
+		unsigned long long* c = R.counters + static_cast<size_t>(L.point) * DMS_NUM_COUNTERS;
+		atomicAdd(c + DMS_CNT_UNFINISHED_TRAJECTORIES, 1ULL);
+		atomicAdd(c + DMS_CNT_UNFINISHED_SCATTERINGS, static_cast<unsigned long long>(L.nscat));
+		atomicAdd(c + DMS_CNT_UNFINISHED_RK_STEPS, static_cast<unsigned long long>(L.steps));
+		atomicAdd(c + DMS_CNT_UNFINISHED_RK_ATTEMPTS, static_cast<unsigned long long>(L.attempts));
+	}
 }
 
 }	// namespace lane

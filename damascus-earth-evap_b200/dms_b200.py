@@ -18,7 +18,9 @@ NUM_HISTS = 8
 COUNTER_NAMES = {0: "trajectories", 1: "free", 2: "reflected", 3: "captured", 4: "completed_outward_escapes",
                  5: "complete_evaporation", 6: "censored_captured", 7: "invalid_survival", 8: "initial_shift_failures",
                  9: "final_reflection_shift_failures", 10: "numerical_failures", 11: "computational_truncations",
-                 12: "total_scatterings", 13: "rk_steps", 14: "events_dropped", 15: "rk_attempts"}
+                 12: "total_scatterings", 13: "rk_steps", 14: "events_dropped", 15: "rk_attempts",
+                 27: "unfinished_trajectories", 28: "unfinished_scatterings", 29: "unfinished_rk_steps",
+                 30: "unfinished_rk_attempts"}
 REASON_BASE = 16
 HIST_NAMES = ["captured_dt", "captured_v2dt", "not_captured_dt", "not_captured_v2dt", "captured_dt_sq",
               "captured_v2dt_sq", "not_captured_dt_sq", "not_captured_v2dt_sq"]

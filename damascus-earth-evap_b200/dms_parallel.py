@@ -14,7 +14,8 @@ import numpy as np
 COUNTER_KEYS = ("trajectories", "free", "reflected", "captured", "completed_outward_escapes", "complete_evaporation",
                 "censored_captured", "invalid_survival", "initial_shift_failures", "final_reflection_shift_failures",
                 "numerical_failures", "computational_truncations", "total_scatterings", "rk_steps", "events_dropped",
-                "rk_attempts")
+                "rk_attempts", "unfinished_trajectories", "unfinished_scatterings", "unfinished_rk_steps",
+                "unfinished_rk_attempts")
 EVENT_DTYPE = [("trajectory_id", np.uint64), ("lifetime_unbinding", np.float64)]
 
 

@@ -234,6 +234,12 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 #define DMS_CNT_EVENTS_DROPPED            14   /* evaporation events beyond the buffer capacity */
 #define DMS_CNT_RK_ATTEMPTS               15   /* RK45 stage evaluations incl. rejected tries (work counter) */
 #define DMS_CNT_REASON_BASE               16   /* + DMS_REASON_*: trajectories per termination reason */
+/* work of the trajectories that a cancelled (time limit) or budget-stopped launch left
+ * unfinished; they are not in any counter above */
+#define DMS_CNT_UNFINISHED_TRAJECTORIES   27
+#define DMS_CNT_UNFINISHED_SCATTERINGS    28
+#define DMS_CNT_UNFINISHED_RK_STEPS       29
+#define DMS_CNT_UNFINISHED_RK_ATTEMPTS    30
 #define DMS_NUM_COUNTERS                  32
 
 /* Histogram slots (each DMS_NUM_BINS doubles), src/Data_Generation.cpp:101-110 */
