@@ -967,30 +967,31 @@ __device__ __forceinline__ double channel_rate(const DevSolar& S, const DevPoint
 
 constexpr int TARGET_FAILED = -2;
 
-// Sample_Target (src/Simulation_Trajectory.cpp:1122-1158) from the channel rates rates[0..62]
-// (isotopes) and rates[63] (electrons): validation, the total in the reference's order, one
-// uniform draw and the cumulative pick.  Returns -1 for an electron, the isotope index, or
-// TARGET_FAILED where the reference throws.
-__device__ __forceinline__ int pick_target(Draws& D, const double* rates)
+// Sample_Target (src/Simulation_Trajectory.cpp:1122-1158) works on the 64 channel rates
+// rates[0..62] (isotopes) and rates[63] (electrons): every rate must be finite and >= 0 (the
+// reference throws otherwise), the total is summed in the reference's order, and one uniform
+// draw picks the channel by the cumulative sum of rate / total.  The result is -1 for an
+// electron, the isotope index, or TARGET_FAILED.
+
+// Total rate: the electron channel plus the 63 isotopes in order.
+__device__ __forceinline__ double channel_total(const double* rates)
 {
-	const double re = rates[DMS_NUM_TARGETS];
-	for(int k = 0; k < DMS_NUM_TARGETS; k++)
-		if(!isfinite(rates[k]) || rates[k] < 0.0)
-			return TARGET_FAILED;
-	if(!isfinite(re) || re < 0.0)
-		return TARGET_FAILED;
-	double total = re;
+	double total = rates[DMS_NUM_TARGETS];
 	for(int k = 0; k < DMS_NUM_TARGETS; k++) total += rates[k];
-	if(!isfinite(total) || total <= 0.0)
-		return TARGET_FAILED;
+	return total;
+}
+
+// The cumulative pick from the fractions q[k] = rate_k / total (q[63] the electrons).
+__device__ __forceinline__ int pick_from_fractions(Draws& D, const double* q)
+{
 	const double xi = D.uniform(0.0, 1.0);
 	int target = -1;
-	double sum = re / total;
+	double sum = q[DMS_NUM_TARGETS];
 	if(!(sum > xi))
 	{
 		for(int k = 0; k < DMS_NUM_TARGETS; k++)
 		{
-			sum += rates[k] / total;
+			sum += q[k];
 			if(sum > xi || k == DMS_NUM_TARGETS - 1)
 			{
 				target = k;
@@ -1000,6 +1001,7 @@ __device__ __forceinline__ int pick_target(Draws& D, const double* rates)
 	}
 	return target;
 }
+
 
 // The rest of Scatter once the target is known: Sample_Target_Velocity, the isotropic
 // scattering angle and New_DM_Velocity, src/Simulation_Trajectory.cpp:1160-1269.  Returns

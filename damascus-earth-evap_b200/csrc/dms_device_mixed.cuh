@@ -77,20 +77,14 @@ __device__ __forceinline__ float gm_f(const DevSolar& S, const DevSolarF& F, flo
 	return __ldg(F.gm + i) + (r - __ldg(F.r + i)) * __ldg(F.gm_s + i);
 }
 
-// J^2/r^3 - G M/r^2 with one reciprocal
-__device__ __forceinline__ float dv_dt_f(float J, float r, float gm)
+// One RK45 stage's derivatives at radius r: dv_r/dt = J^2/r^3 - G M/r^2 (r clamped to >= 1 km)
+// and dphi/dt = J/r^2, from one reciprocal.
+__device__ __forceinline__ void stage_rates(const PropF& p, float r, float gm, float& dv, float& dp)
 {
-	r = r < 1.0f ? 1.0f : r;
-	const float inv = __frcp_rn(r);
-	return (J * J * inv - gm) * inv * inv;
-}
-
-__device__ __forceinline__ float dphi_dt_f(const PropF& p, float r)
-{
-	if(p.radial_mode || p.J == 0.0f || r <= 0.0f)
-		return 0.0f;
-	const float inv = __frcp_rn(r);
-	return p.J * inv * inv;
+	const float inv = 1.0f / fmaxf(r, 1.0f);
+	const float inv2 = inv * inv;
+	dv = (p.J * p.J * inv - gm) * inv2;
+	dp = (p.radial_mode || p.J == 0.0f || r <= 0.0f) ? 0.0f : p.J * inv2;
 }
 
 // One pass of the Runge_Kutta_45_Step retry loop (src/Simulation_Trajectory.cpp:1492-1600):
@@ -99,30 +93,35 @@ __device__ __forceinline__ int rk45_attempt_f(const DevSolar& S, const DevSolarF
 {
 	const float dt = static_cast<float>(p.time_step);
 	const float r = static_cast<float>(p.radius), v = static_cast<float>(p.v_radial);
-	const float J = p.J;
-	float kr0, kr1, kr2, kr3, kr4, kr5, kv0, kv1, kv2, kv3, kv4, kv5, kp0, kp2, kp3, kp4, kp5, ri;
+	float kr0, kr1, kr2, kr3, kr4, kr5, kv0, kv1, kv2, kv3, kv4, kv5, kp0, kp2, kp3, kp4, kp5, ri, a, b;
+	stage_rates(p, r, gm_f(S, F, r), a, b);
 	kr0 = dt * v;
-	kv0 = dt * dv_dt_f(J, r, gm_f(S, F, r));
-	kp0 = dt * dphi_dt_f(p, r);
+	kv0 = dt * a;
+	kp0 = dt * b;
 	ri = r + 0.25f * kr0;
 	kr1 = dt * (v + 0.25f * kv0);
-	kv1 = dt * dv_dt_f(J, ri, gm_f(S, F, ri));
+	stage_rates(p, ri, gm_f(S, F, ri), a, b);
+	kv1 = dt * a;  // stage 1's dphi has no weight in either solution
 	ri = r + (3.0f / 32.0f) * kr0 + (9.0f / 32.0f) * kr1;
 	kr2 = dt * (v + (3.0f / 32.0f) * kv0 + (9.0f / 32.0f) * kv1);
-	kv2 = dt * dv_dt_f(J, ri, gm_f(S, F, ri));
-	kp2 = dt * dphi_dt_f(p, ri);
+	stage_rates(p, ri, gm_f(S, F, ri), a, b);
+	kv2 = dt * a;
+	kp2 = dt * b;
 	ri = r + (1932.0f / 2197.0f) * kr0 - (7200.0f / 2197.0f) * kr1 + (7296.0f / 2197.0f) * kr2;
 	kr3 = dt * (v + (1932.0f / 2197.0f) * kv0 - (7200.0f / 2197.0f) * kv1 + (7296.0f / 2197.0f) * kv2);
-	kv3 = dt * dv_dt_f(J, ri, gm_f(S, F, ri));
-	kp3 = dt * dphi_dt_f(p, ri);
+	stage_rates(p, ri, gm_f(S, F, ri), a, b);
+	kv3 = dt * a;
+	kp3 = dt * b;
 	ri = r + (439.0f / 216.0f) * kr0 - 8.0f * kr1 + (3680.0f / 513.0f) * kr2 - (845.0f / 4104.0f) * kr3;
 	kr4 = dt * (v + (439.0f / 216.0f) * kv0 - 8.0f * kv1 + (3680.0f / 513.0f) * kv2 - (845.0f / 4104.0f) * kv3);
-	kv4 = dt * dv_dt_f(J, ri, gm_f(S, F, ri));
-	kp4 = dt * dphi_dt_f(p, ri);
+	stage_rates(p, ri, gm_f(S, F, ri), a, b);
+	kv4 = dt * a;
+	kp4 = dt * b;
 	ri = r - (8.0f / 27.0f) * kr0 + 2.0f * kr1 - (3544.0f / 2565.0f) * kr2 + (1859.0f / 4104.0f) * kr3 - (11.0f / 40.0f) * kr4;
 	kr5 = dt * (v - (8.0f / 27.0f) * kv0 + 2.0f * kv1 - (3544.0f / 2565.0f) * kv2 + (1859.0f / 4104.0f) * kv3 - (11.0f / 40.0f) * kv4);
-	kv5 = dt * dv_dt_f(J, ri, gm_f(S, F, ri));
-	kp5 = dt * dphi_dt_f(p, ri);
+	stage_rates(p, ri, gm_f(S, F, ri), a, b);
+	kv5 = dt * a;
+	kp5 = dt * b;
 	// 4th-order increments (FP32) and the 5th - 4th order difference in FP64
 	const float dr4 = (25.0f / 216.0f) * kr0 + (1408.0f / 2565.0f) * kr2 + (2197.0f / 4104.0f) * kr3 - 0.2f * kr4;
 	const float dv4 = (25.0f / 216.0f) * kv0 + (1408.0f / 2565.0f) * kv2 + (2197.0f / 4104.0f) * kv3 - 0.2f * kv4;
@@ -400,6 +399,148 @@ __device__ __forceinline__ EventF interpolate_event_f(const EventF& a, const Eve
 	e.v = f3(a.v.x + f * (b.v.x - a.v.x), a.v.y + f * (b.v.y - a.v.y), a.v.z + f * (b.v.z - a.v.z));
 	e.t = a.t + static_cast<double>(f) * (b.t - a.t);
 	return e;
+}
+
+// ---- scattering in FP32 (the energy that decides capture stays FP64 in the caller) ----------
+
+// Thermal_Averaged_Relative_Speed (src/Solar_Model.cpp:493-521) in FP32
+__device__ __forceinline__ float thermal_relative_speed_f(float T, float m, float v)
+{
+	const float sqrt_pi = 1.7724538509055159f;
+	if(!isfinite(T) || T <= 0.0f || !isfinite(m) || m <= 0.0f || !isfinite(v) || v < 0.0f)
+		return NAN;
+	const float kappa = sqrtf(m / (2.0f * T)) / static_cast<float>(DMS_C_KMS);
+	if(!isfinite(kappa) || kappa <= 0.0f)
+		return NAN;
+	if(v == 0.0f)
+		return 2.0f / sqrt_pi / kappa;
+	const float x = kappa * v;
+	if(!isfinite(x))
+		return v;
+	const float x2 = x * x;
+	if(x < 1.0e-4f)
+		return 2.0f / sqrt_pi / kappa * (1.0f + x2 / 3.0f - x2 * x2 / 30.0f + x2 * x2 * x2 / 210.0f);
+	if(x > 26.0f)
+		return v * (1.0f + 0.5f / x2);
+	return v * ((1.0f + 2.0f * x2) * erff(x) / (2.0f * x2) + expf(-x2) / (sqrt_pi * x));
+}
+
+// One channel of Total_DM_Scattering_Rate_Computed (src/Solar_Model.cpp:263-303): density
+// times cross section in FP64 (the factors alone exceed the FP32 range), the thermal average
+// in FP32.  k == DMS_NUM_TARGETS is the electron channel.
+__device__ __forceinline__ double channel_rate_f(const DevSolar& S, const DevPoint* __restrict__ P, int i, double dr, double T, double v, int k)
+{
+	double n_sigma;
+	float m;
+	if(k == DMS_NUM_TARGETS)
+	{
+		n_sigma = (__ldg(S.ne + i) + dr * __ldg(S.ne_s + i)) * __ldg(&P->sigma_e);
+		m = static_cast<float>(DMS_MELECTRON_GEV);
+	}
+	else
+	{
+		const size_t o = static_cast<size_t>(i) * DMS_NUM_TARGETS + k;
+		n_sigma = (__ldg(S.nt + o) + dr * __ldg(S.nt_s + o)) * __ldg(&P->sigma_t[k]);
+		m = static_cast<float>(__ldg(S.target_mass + k));
+	}
+	return n_sigma * static_cast<double>(thermal_relative_speed_f(static_cast<float>(T), m, static_cast<float>(v)));
+}
+
+// Unit_Vector_At_Angle_From_Axis (src/Simulation_Trajectory.cpp:109-128) in FP32
+__device__ __forceinline__ bool unit_vector_at_angle_f(float cos_theta, float phi, const F3& axis, F3& out)
+{
+	if(!isfinite(cos_theta) || cos_theta < -1.0f - 1.0e-6f || cos_theta > 1.0f + 1.0e-6f || !isfinite(phi))
+		return false;
+	const float n = normf(axis);
+	if(!isfinite(n) || n <= 0.0f)
+		return false;
+	const F3 e3 = f3(axis.x / n, axis.y / n, axis.z / n);
+	const F3 ref = (fabsf(e3.z) < 0.9f) ? f3(0.0f, 0.0f, 1.0f) : f3(1.0f, 0.0f, 0.0f);
+	F3 e1 = f3(ref.y * e3.z - ref.z * e3.y, ref.z * e3.x - ref.x * e3.z, ref.x * e3.y - ref.y * e3.x);
+	const float n1 = normf(e1);
+	e1 = f3(e1.x / n1, e1.y / n1, e1.z / n1);
+	const F3 e2 = f3(e3.y * e1.z - e3.z * e1.y, e3.z * e1.x - e3.x * e1.z, e3.x * e1.y - e3.y * e1.x);
+	cos_theta = fminf(fmaxf(cos_theta, -1.0f), 1.0f);
+	const float st = sqrtf(fmaxf(1.0f - cos_theta * cos_theta, 0.0f));
+	float sp, cp;
+	sincosf(phi, &sp, &cp);
+	out = f3(cos_theta * e3.x + st * cp * e1.x + st * sp * e2.x, cos_theta * e3.y + st * cp * e1.y + st * sp * e2.y,
+	         cos_theta * e3.z + st * cp * e1.z + st * sp * e2.z);
+	return true;
+}
+
+// Scatter once the target is known, in FP32: Sample_Target_Velocity (free-gas rejection),
+// the isotropic angle and New_DM_Velocity, src/Simulation_Trajectory.cpp:1160-1269.  Same draw
+// sequence as the FP64 form.  Returns false where the reference throws.
+static __device__ __noinline__ bool scatter_with_target_f(const DevSolar& S, const DevPoint* __restrict__ P, Draws& D, Event& e, int target)
+{
+	const double r = ev_radius(e);
+	const float m_target = target < 0 ? static_cast<float>(DMS_MELECTRON_GEV) : static_cast<float>(__ldg(S.target_mass + target));
+	const float T = static_cast<float>(solar_temperature(S, r));
+	if(!isfinite(T) || T <= 0.0f || !isfinite(m_target) || m_target <= 0.0f)
+		return false;
+	const float kappa = sqrtf(m_target / 2.0f / T) / static_cast<float>(DMS_C_KMS);
+	const F3 vd = f3(static_cast<float>(e.v.x), static_cast<float>(e.v.y), static_cast<float>(e.v.z));
+	const float vdm = normf(vd);
+	if(!isfinite(kappa) || kappa <= 0.0f || !isfinite(vdm) || vdm <= 0.0f)
+		return false;
+	const float y = kappa * vdm;
+	const float sqrt_pi = 1.7724538509055159f;
+	float x = y, mu = 1.0f;
+	unsigned long attempts = 0;
+	for(;;)
+	{
+		const float raw = x * x + y * y - 2.0f * x * y * mu;
+		const float den = x + y;
+		if(!isfinite(x) || x < 0.0f || !isfinite(mu) || !isfinite(raw) || !isfinite(den) || den <= 0.0f)
+			return false;
+		const float ratio = sqrtf(fmaxf(raw, 0.0f)) / den;
+		const float accept = ratio < 1.0f ? ratio : 1.0f;
+		if(!(static_cast<double>(accept) < D.uniform(0.0, 1.0)))
+			break;
+		attempts++;
+		if(attempts > DMS_TARGET_VELOCITY_MAX_REJECTIONS)
+			return false;
+		mu = static_cast<float>(D.uniform(-1.0, 1.0));
+		const double xi1 = D.uniform(0.0, 1.0);
+		if(xi1 < static_cast<double>(2.0f / (sqrt_pi * y + 2.0f)))
+		{
+			const float xi2 = static_cast<float>(D.positive_unit());
+			const float xi3 = static_cast<float>(D.positive_unit());
+			x = sqrtf(-logf(xi2) - logf(xi3));
+		}
+		else
+		{
+			const float xi2 = static_cast<float>(D.positive_unit());
+			const float xi3 = static_cast<float>(D.uniform(0.0, 1.0));
+			const float xi4 = static_cast<float>(D.positive_unit());
+			const float c = cosf(1.5707963267948966f * xi3);
+			x = sqrtf(-logf(xi2) - (c * c) * logf(xi4));
+		}
+	}
+	const float vT = x / kappa;
+	const float phi_t = static_cast<float>(D.uniform(0.0, 2.0 * DMS_PI));
+	F3 unit_t;
+	if(!unit_vector_at_angle_f(mu, phi_t, vd, unit_t))
+		return false;
+	const F3 vel_t = f3(vT * unit_t.x, vT * unit_t.y, vT * unit_t.z);
+	const float cos_alpha = static_cast<float>(D.uniform(-1.0, 1.0));
+	const float md = static_cast<float>(__ldg(&P->m_dm));
+	if(!isfinite(normf(vel_t)) || !isfinite(md) || md <= 0.0f)
+		return false;
+	const float phi_n = static_cast<float>(D.uniform(0.0, 2.0 * DMS_PI));
+	F3 n;
+	if(!unit_vector_at_angle_f(fminf(fmaxf(cos_alpha, -1.0f), 1.0f), phi_n, vd, n))
+		return false;
+	const F3 rel = f3(vel_t.x - vd.x, vel_t.y - vd.y, vel_t.z - vd.z);
+	const float inv_m = 1.0f / (m_target + md);
+	const float sc = m_target * normf(rel) * inv_m;
+	const F3 out = f3(sc * n.x + (md * vd.x + m_target * vel_t.x) * inv_m, sc * n.y + (md * vd.y + m_target * vel_t.y) * inv_m,
+	                  sc * n.z + (md * vd.z + m_target * vel_t.z) * inv_m);
+	if(!isfinite(normf(out)))
+		return false;
+	e.v = mk(out.x, out.y, out.z);
+	return true;
 }
 
 }	// namespace mixed

@@ -357,6 +357,14 @@ struct StrictStep
 	{
 		return free_step(R, P, m_dm, L, hist);
 	}
+	__device__ __forceinline__ double channel(const DevSolar& S, const DevPoint* __restrict__ P, int i, double dr, double T, double v, int k) const
+	{
+		return channel_rate(S, P, i, dr, T, v, k);
+	}
+	__device__ __forceinline__ bool scatter(const DevSolar& S, const DevPoint* __restrict__ P, Draws& D, Event& e, int target) const
+	{
+		return scatter_with_target(S, P, D, e, target);
+	}
 };
 
 __global__ void __launch_bounds__(128, DMS_TRAJ_MIN_BLOCKS) trajectory_kernel(const RunParams R)

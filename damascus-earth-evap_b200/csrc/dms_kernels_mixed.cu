@@ -106,8 +106,12 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 				set_final(L, to_event64(prop_event_f(L.pr)), true, DMS_REASON_NUMERICAL_FAILURE);
 				return PH_FINAL;
 			}
-			if(L.rate_before > 0.0 && tau_limit / L.rate_before < L.pr.time_step)
-				L.pr.time_step = tau_limit / L.rate_before;
+			if(L.rate_before > 0.0)
+			{
+				const float lim = static_cast<float>(tau_limit) / static_cast<float>(L.rate_before);
+				if(static_cast<double>(lim) < L.pr.time_step)
+					L.pr.time_step = static_cast<double>(lim);
+			}
 		}
 		// the RK step changes only these propagator fields
 		L.b_time = L.pr.time;
@@ -156,10 +160,11 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 		const int pieces = capture_mode ? DMS_CAPTURE_OPTICAL_DEPTH_PIECES : DMS_MAX_OPTICAL_DEPTH_PIECES;
 		const bool use_cached = r_before < DMS_RSUN_KM && s0 <= 1.0e-12f;
 		const float span = s1 - s0;
+		const float adt = static_cast<float>(actual_dt);
 		float fr[DMS_MAX_OPTICAL_DEPTH_PIECES + 1];
-		double rt[DMS_MAX_OPTICAL_DEPTH_PIECES + 1];
+		float rt[DMS_MAX_OPTICAL_DEPTH_PIECES + 1];
 		bool invalid = false;
-		double dtau = 0.0, tau2 = 0.0;
+		float dtau_f = 0.0f, tau2 = 0.0f;  // optical depths of one step (<= 0.1) in FP32
 		if(s1 > s0 && actual_dt > 0.0)
 		{
 #pragma unroll
@@ -168,28 +173,29 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 				if(i > pieces)
 					break;
 				fr[i] = s0 + static_cast<float>(i) / static_cast<float>(pieces) * span;
-				rt[i] = (i == 0 && use_cached) ? rate_before : static_cast<double>(rate_at_fraction_f(S, P, grid, before, after, fr[i]));
-				if(!isfinite(rt[i]) || rt[i] < 0.0)
+				rt[i] = (i == 0 && use_cached) ? static_cast<float>(rate_before) : rate_at_fraction_f(S, P, grid, before, after, fr[i]);
+				if(!isfinite(rt[i]) || rt[i] < 0.0f)
 					invalid = true;
 			}
 			if(!invalid)
 			{
 				if(pieces >= 4)
-					tau2 = 0.5 * (rt[0] + rt[2]) * (actual_dt * static_cast<double>(fr[2] - fr[0])) + 0.5 * (rt[2] + rt[4]) * (actual_dt * static_cast<double>(fr[4] - fr[2]));
+					tau2 = 0.5f * (rt[0] + rt[2]) * (adt * (fr[2] - fr[0])) + 0.5f * (rt[2] + rt[4]) * (adt * (fr[4] - fr[2]));
 				else
-					for(int i = 0; i < pieces; i++) tau2 += 0.5 * (rt[i] + rt[i + 1]) * (actual_dt * static_cast<double>(fr[i + 1] - fr[i]));
+					for(int i = 0; i < pieces; i++) tau2 += 0.5f * (rt[i] + rt[i + 1]) * (adt * (fr[i + 1] - fr[i]));
 				for(int i = 0; i < pieces; i++)
 					if(fr[i + 1] > fr[i])
-						dtau += 0.5 * (rt[i] + rt[i + 1]) * (actual_dt * static_cast<double>(fr[i + 1] - fr[i]));
+						dtau_f += 0.5f * (rt[i] + rt[i + 1]) * (adt * (fr[i + 1] - fr[i]));
 			}
 		}
+		const double dtau = static_cast<double>(dtau_f);
 		if(invalid || !isfinite(dtau) || dtau < 0.0)
 		{
 			set_final(L, to_event64(after), true, DMS_REASON_NUMERICAL_FAILURE);
 			return PH_FINAL;
 		}
-		const double scale = dtau > DMS_OPTICAL_DEPTH_ABS_TOL ? dtau : DMS_OPTICAL_DEPTH_ABS_TOL;
-		const double rel = fabs(dtau - tau2) / scale;
+		const float scale = dtau_f > static_cast<float>(DMS_OPTICAL_DEPTH_ABS_TOL) ? dtau_f : static_cast<float>(DMS_OPTICAL_DEPTH_ABS_TOL);
+		const double rel = static_cast<double>(fabsf(dtau_f - tau2) / scale);
 		const bool reject_depth = dtau > tau_limit;
 		const bool reject_acc = !capture_mode && rel > DMS_OPTICAL_DEPTH_REL_TOL;
 		if(reject_depth || reject_acc)
@@ -223,7 +229,7 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 				if(!(fr[k + 1] > fr[k]))
 					continue;
 				const double pdt = actual_dt * static_cast<double>(fr[k + 1] - fr[k]);
-				const double ptau = 0.5 * (rt[k] + rt[k + 1]) * pdt;
+				const double ptau = 0.5 * static_cast<double>(rt[k] + rt[k + 1]) * pdt;
 				if(ptau >= remaining)
 				{
 					const double lf = solve_linear_rate(rt[k], rt[k + 1], pdt, remaining);
@@ -330,6 +336,14 @@ struct MixedStep
 	__device__ __forceinline__ int operator()(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, MixedLane& L, double2* hist) const
 	{
 		return free_step_mixed(R, P, m_dm, L, hist);
+	}
+	__device__ __forceinline__ double channel(const DevSolar& S, const DevPoint* __restrict__ P, int i, double dr, double T, double v, int k) const
+	{
+		return channel_rate_f(S, P, i, dr, T, v, k);
+	}
+	__device__ __forceinline__ bool scatter(const DevSolar& S, const DevPoint* __restrict__ P, Draws& D, Event& e, int target) const
+	{
+		return scatter_with_target_f(S, P, D, e, target);
 	}
 };
 

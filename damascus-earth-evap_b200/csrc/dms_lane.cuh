@@ -538,8 +538,8 @@ __device__ __forceinline__ int start_trajectory(const RunParams& R, Lane& L, uin
 // scattering lane then validates, sums and picks sequentially in the reference's order, so
 // the target and the draws consumed are those of the one-lane form.  `rates` is this warp's
 // DMS_NUM_TARGETS + 1 doubles of shared memory.
-template <class Lane>
-__device__ __forceinline__ void cooperative_targets(const RunParams& R, Lane& L, int phase, double* rates, int& target)
+template <class Lane, class Step>
+__device__ __forceinline__ void cooperative_targets(const RunParams& R, Lane& L, int phase, double* rates, int& target, const Step& step)
 {
 	const unsigned int grp = __activemask();
 	unsigned int pending = __ballot_sync(grp, phase == PH_SCATTER);
@@ -558,28 +558,45 @@ __device__ __forceinline__ void cooperative_targets(const RunParams& R, Lane& L,
 		const double r = __shfl_sync(grp, my_r, leader);
 		const double v = __shfl_sync(grp, my_v, leader);
 		const int point = __shfl_sync(grp, L.point, leader);
-		if(isfinite(r) && isfinite(v))
+		bool bad = !(isfinite(r) && isfinite(v));
+		if(!bad)
 		{
 			const DevPoint* P = R.points + point;
 			const int i = knot_index(R.S, r);
 			const double dr = r - __ldg(R.S.r + i);
 			const double T = __ldg(R.S.temp + i) + dr * __ldg(R.S.temp_s + i);
 			for(int k = rank; k <= DMS_NUM_TARGETS; k += size)
-				rates[k] = channel_rate(R.S, P, i, dr, T, v, k);
+			{
+				const double x = step.channel(R.S, P, i, dr, T, v, k);
+				bad = bad || !(isfinite(x) && x >= 0.0);
+				rates[k] = x;
+			}
 		}
+		// validation: every channel finite and >= 0 (the reference throws otherwise)
+		bad = __any_sync(grp, bad);
+		__syncwarp(grp);
+		double total = 0.0;
+		if(me == leader && !bad)
+			total = channel_total(rates);
+		total = __shfl_sync(grp, total, leader);
+		const bool ok = !bad && isfinite(total) && total > 0.0;
+		// the 64 divisions by the total, in parallel: each lane replaces its channels by
+		// their fractions, exactly the quotients the sequential pick forms
+		if(ok)
+			for(int k = rank; k <= DMS_NUM_TARGETS; k += size) rates[k] = rates[k] / total;
 		__syncwarp(grp);
 		if(me == leader)
-			target = (isfinite(r) && isfinite(v)) ? pick_target(L.D, rates) : TARGET_FAILED;
+			target = ok ? pick_from_fractions(L.D, rates) : TARGET_FAILED;
 		__syncwarp(grp);
 	}
 }
 
 // Simulate after a scattering point (src/Simulation_Trajectory.cpp:1313-1346): target
 // velocity, angle and kinematics, then capture bookkeeping and the bincount anchor.
-template <class Lane>
-__device__ __forceinline__ int finish_scatter(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, Lane& L, int target)
+template <class Lane, class Step>
+__device__ __forceinline__ int finish_scatter(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, Lane& L, int target, const Step& step)
 {
-	if(target == TARGET_FAILED || !scatter_with_target(R.S, P, L.D, L.cur, target))
+	if(target == TARGET_FAILED || !step.scatter(R.S, P, L.D, L.cur, target))
 	{
 		L.reason = DMS_REASON_NUMERICAL_FAILURE;
 		return PH_FINAL;
@@ -602,6 +619,13 @@ __device__ __forceinline__ int finish_scatter(const RunParams& R, const DevPoint
 	return PH_SEGMENT;
 }
 
+#ifndef DMS_SCATTER_BATCH
+#define DMS_SCATTER_BATCH 8
+#endif
+#ifndef DMS_SCATTER_MAX_WAIT
+#define DMS_SCATTER_MAX_WAIT 16
+#endif
+
 template <class Lane, class Step>
 __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 {
@@ -616,6 +640,7 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	const DevPoint* P = R.points;
 	double m_dm = 0.0;
 	int phase = PH_FETCH;
+	int scatter_wait = 0;
 	const unsigned int lane_bit = 1u << (threadIdx.x & 31);
 	for(uint64_t iter = 0;; iter++)
 	{
@@ -651,10 +676,31 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 			phase = segment_start(R, P, m_dm, L);
 		if(phase == PH_STEP)
 			phase = step(R, P, m_dm, L, hist);
-		int target = TARGET_FAILED;
-		cooperative_targets(R, L, phase, rates, target);
-		if(phase == PH_SCATTER)
-			phase = finish_scatter(R, P, m_dm, L, target);
+		// Scatterings wait until several lanes of the warp have one (or one has waited
+		// DMS_SCATTER_MAX_WAIT iterations, or no lane is stepping), so that the scattering code
+		// runs for many lanes at once.  A lane's draws do not depend on when it scatters.
+		{
+			const unsigned int grp = __activemask();
+			const unsigned int waiting = __ballot_sync(grp, phase == PH_SCATTER);
+			if(waiting != 0u)
+			{
+				const unsigned int stepping = __ballot_sync(grp, phase == PH_STEP);
+				const bool go = __popc(waiting) >= DMS_SCATTER_BATCH || stepping == 0u ||
+				                __any_sync(grp, phase == PH_SCATTER && scatter_wait >= DMS_SCATTER_MAX_WAIT);
+				if(go)
+				{
+					int target = TARGET_FAILED;
+					cooperative_targets(R, L, phase, rates, target, step);
+					if(phase == PH_SCATTER)
+					{
+						phase = finish_scatter(R, P, m_dm, L, target, step);
+						scatter_wait = 0;
+					}
+				}
+				else if(phase == PH_SCATTER)
+					scatter_wait++;
+			}
+		}
 		if(phase == PH_FINAL)
 		{
 			write_back_bin(L, hist);
