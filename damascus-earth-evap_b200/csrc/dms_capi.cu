@@ -513,12 +513,15 @@ int dms_add_point(dms_ctx* ctx, const dms_point_params* params, int* point_id)
 		return rc;
 	double* grid = nullptr;
 	float* grid_f = nullptr;
-	DMS_CUDA(ctx, cudaMalloc(&grid, sizeof(double) * c.grid_n * c.grid_n));
-	const cudaError_t e0 = cudaMalloc(&grid_f, sizeof(float) * c.grid_n * c.grid_n);
-	if(e0 != cudaSuccess)
+	if(c.grid_n > 0)  // interpolation_points < 2: no grid, rates are computed per lookup
 	{
-		cudaFree(grid);
-		return Fail(ctx, DMS_ERR_CUDA, cudaGetErrorString(e0));
+		DMS_CUDA(ctx, cudaMalloc(&grid, sizeof(double) * c.grid_n * c.grid_n));
+		const cudaError_t e0 = cudaMalloc(&grid_f, sizeof(float) * c.grid_n * c.grid_n);
+		if(e0 != cudaSuccess)
+		{
+			cudaFree(grid);
+			return Fail(ctx, DMS_ERR_CUDA, cudaGetErrorString(e0));
+		}
 	}
 	DevPoint d;
 	Fill_Dev_Point(c, grid, d);
@@ -530,7 +533,8 @@ int dms_add_point(dms_ctx* ctx, const dms_point_params* params, int* point_id)
 		cudaFree(grid_f);
 		return Fail(ctx, DMS_ERR_CUDA, cudaGetErrorString(e1));
 	}
-	Launch_Rate_Grid(ctx->dsolar, ctx->d_points + id, grid, c.grid_n, ctx->stream);
+	if(c.grid_n > 0)
+		Launch_Rate_Grid(ctx->dsolar, ctx->d_points + id, grid, c.grid_n, ctx->stream);
 	const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
 	if(e2 != cudaSuccess || cudaGetLastError() != cudaSuccess)
 	{
@@ -541,7 +545,7 @@ int dms_add_point(dms_ctx* ctx, const dms_point_params* params, int* point_id)
 	ctx->points.push_back(c);
 	ctx->d_grids.push_back(grid);
 	ctx->d_grids_f.push_back(grid_f);
-	ctx->grid_f_valid.push_back(0);
+	ctx->grid_f_valid.push_back(c.grid_n > 0 ? 0 : 1);
 	DMS_CUDA(ctx, cudaMemset(ctx->d_counters + static_cast<size_t>(id) * DMS_NUM_COUNTERS, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_hists + static_cast<size_t>(id) * DMS_NUM_HISTS * DMS_NUM_BINS, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_event_count + id, 0, sizeof(unsigned long long)));
@@ -558,6 +562,8 @@ int dms_set_rate_grid(dms_ctx* ctx, int point_id, const double* grid, uint32_t n
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
 	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
 		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	if(ctx->points[point_id].grid_n == 0)
+		return Fail(ctx, DMS_ERR_STATE, "the point has no rate grid (interpolation_points < 2)");
 	if(static_cast<int>(n) != ctx->points[point_id].grid_n)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "grid size does not match the point's interpolation_points");
 	DMS_CUDA(ctx, cudaMemcpy(ctx->d_grids[point_id], grid, sizeof(double) * n * n, cudaMemcpyHostToDevice));
@@ -571,6 +577,8 @@ int dms_get_rate_grid(dms_ctx* ctx, int point_id, double* grid, uint32_t n)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
 	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
 		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	if(ctx->points[point_id].grid_n == 0)
+		return Fail(ctx, DMS_ERR_STATE, "the point has no rate grid (interpolation_points < 2)");
 	if(static_cast<int>(n) != ctx->points[point_id].grid_n)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "grid size does not match the point's interpolation_points");
 	DMS_CUDA(ctx, cudaMemcpy(grid, ctx->d_grids[point_id], sizeof(double) * n * n, cudaMemcpyDeviceToHost));

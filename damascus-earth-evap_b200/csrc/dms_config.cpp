@@ -363,10 +363,6 @@ std::string Load_Run_Config(const std::string& path, RunConfig& cfg)
 			return "Error: 'SHM_vObserver' must be a list of three velocities.";
 		for(int i = 0; i < 3; i++) cfg.vobs[i] = v->items[i].number;
 	}
-	if(cfg.interpolation_points == 0)
-		return "Error: interpolation_points = 0 (direct rate evaluation per step) is not provided by this engine; set interpolation_points >= 2.";
-	if(cfg.interpolation_points < 2)
-		return "Error: interpolation_points must be at least 2.";
 	return "";
 }
 

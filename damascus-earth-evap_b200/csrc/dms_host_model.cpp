@@ -252,8 +252,6 @@ std::string Make_Point_Constants(const SolarTables& t, const dms_point_params& p
 		return "DM mass must be finite and positive";
 	if(!(p.sigma_p_cm2 >= 0.0) || !std::isfinite(p.sigma_p_cm2) || !(p.sigma_e_cm2 >= 0.0) || !std::isfinite(p.sigma_e_cm2))
 		return "DM cross sections must be finite and non-negative";
-	if(p.interpolation_points < 2)
-		return "interpolation_points must be at least 2 (the direct-rate path is not built)";
 	if(static_cast<uint64_t>(p.interpolation_points) * p.interpolation_points > (1ULL << 28))
 		return "interpolation grid too large";
 	if(!(p.halo_v0_kms > 0.0) || !(p.halo_vesc_kms > 0.0))
@@ -285,6 +283,17 @@ std::string Make_Point_Constants(const SolarTables& t, const dms_point_params& p
 	c.avg_speed = Halo_Moment(c, 1, 0.0, c.vesc_halo - c.vobs) + Halo_Moment(c, 1, c.vesc_halo - c.vobs, c.vesc_halo + c.vobs);
 	c.eta0 = Halo_Moment(c, -1, 0.0, c.vesc_halo - c.vobs) + Halo_Moment(c, -1, c.vesc_halo - c.vobs, c.vesc_halo + c.vobs);
 	const unsigned int N = p.interpolation_points;
+	if(N < 2)
+	{
+		// no grid (Interpolate_Total_DM_Scattering_Rate with N < 2, src/Solar_Model.cpp:397-405):
+		// every lookup is Total_DM_Scattering_Rate_Computed; a negative limit speed sends every
+		// speed to that branch
+		c.grid_n = 0;
+		c.grid_inv_r = 0.0;
+		c.grid_inv_v = 0.0;
+		c.grid_vmax = -1.0;
+		return "";
+	}
 	c.grid_n = static_cast<int>(N);
 	c.grid_inv_r = static_cast<double>(N - 1) / DMS_RSUN_KM;
 	c.grid_vmax = DMS_V_MAX_C * DMS_C_KMS;

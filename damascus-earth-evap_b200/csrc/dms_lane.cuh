@@ -625,6 +625,12 @@ __device__ __forceinline__ int finish_scatter(const RunParams& R, const DevPoint
 #ifndef DMS_SCATTER_MAX_WAIT
 #define DMS_SCATTER_MAX_WAIT 16
 #endif
+#ifndef DMS_FINAL_BATCH
+#define DMS_FINAL_BATCH 1
+#endif
+#ifndef DMS_FINAL_MAX_WAIT
+#define DMS_FINAL_MAX_WAIT 16
+#endif
 
 template <class Lane, class Step>
 __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
@@ -641,6 +647,7 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	double m_dm = 0.0;
 	int phase = PH_FETCH;
 	int scatter_wait = 0;
+	int final_wait = 0;
 	const unsigned int lane_bit = 1u << (threadIdx.x & 31);
 	for(uint64_t iter = 0;; iter++)
 	{
@@ -701,13 +708,30 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 					scatter_wait++;
 			}
 		}
-		if(phase == PH_FINAL)
+		// terminations are batched the same way
 		{
-			write_back_bin(L, hist);
-			finalize(R, P, m_dm, L, job);
-			phase = PH_FETCH;
+			const unsigned int grp = __activemask();
+			const unsigned int ending = __ballot_sync(grp, phase == PH_FINAL);
+			if(ending != 0u)
+			{
+				const unsigned int stepping = __ballot_sync(grp, phase == PH_STEP);
+				const bool go = __popc(ending) >= DMS_FINAL_BATCH || stepping == 0u ||
+				                __any_sync(grp, phase == PH_FINAL && final_wait >= DMS_FINAL_MAX_WAIT);
+				if(go)
+				{
+					if(phase == PH_FINAL)
+					{
+						write_back_bin(L, hist);
+						finalize(R, P, m_dm, L, job);
+						phase = PH_FETCH;
+						final_wait = 0;
+					}
+					cooperative_flush(hist, job);
+				}
+				else if(phase == PH_FINAL)
+					final_wait++;
+			}
 		}
-		cooperative_flush(hist, job);
 	}
 	if(phase != PH_FETCH && L.bmax >= L.bmin)
 		for(int b = L.bmin; b <= L.bmax; b++) hist[b] = make_double2(0.0, 0.0);

@@ -129,7 +129,8 @@ typedef struct
 	double halo_v0_kms;                /* SHM_v0 */
 	double halo_vesc_kms;              /* SHM_vEscape */
 	double halo_vobs_kms[3];           /* SHM_vObserver */
-	uint32_t interpolation_points;     /* N of the N x N total-rate grid; must be >= 2 */
+	uint32_t interpolation_points;     /* N of the N x N total-rate grid; N < 2: no grid, every
+	                                      lookup sums the 64 channels (Total_DM_Scattering_Rate_Computed) */
 	uint32_t reserved;
 } dms_point_params;
 

@@ -1915,7 +1915,7 @@ const char* dms_oracle_last_error(const dms_oracle* o) { return o ? o->error : "
 
 int dms_oracle_set_point(dms_oracle* o, const dms_point_params* p)
 {
-	if(!o || !p || p->interpolation_points < 2 || !(p->mass_gev > 0.0))
+	if(!o || !p || !(p->mass_gev > 0.0))
 		return DMS_ERR_INVALID_ARGUMENT;
 	o->m_dm = p->mass_gev;
 	const double sigma_p = p->sigma_p_cm2 * 1.0e-10;
@@ -1942,6 +1942,17 @@ int dms_oracle_set_point(dms_oracle* o, const dms_point_params* p)
 	/* rate grid, Interpolate_Total_DM_Scattering_Rate src/Solar_Model.cpp:395-465 */
 	const unsigned int N = p->interpolation_points;
 	free(o->grid);
+	o->grid = NULL;
+	if(N < 2)
+	{
+		/* N < 2: no grid, every lookup is computed (src/Solar_Model.cpp:397-405) */
+		o->grid_n = 0;
+		o->grid_inv_r = 0.0;
+		o->grid_inv_v = 0.0;
+		o->grid_vmax = -1.0;
+		o->has_point = 1;
+		return DMS_OK;
+	}
 	o->grid = (double*)malloc((size_t)N * N * sizeof(double));
 	if(!o->grid)
 		return DMS_ERR_CAPACITY;

@@ -1,0 +1,117 @@
+"""The `dms_sun` command-line drop-in: configuration errors (CPU, the file is read before any
+CUDA call) and complete Parameter-point and Capture runs with their summary and output files
+(B200 required)."""
+import os
+import subprocess
+
+import pytest
+
+from dms_ctypes import PACKAGE_DIR
+
+DMS_SUN = os.path.join(PACKAGE_DIR, "dms_sun")
+
+BASE = {
+    "ID": '"cli_test"',
+    "run_mode": '"Parameter point"',
+    "sample_size": "16",
+    "fixed_seed": "7",
+    "max_trajectories": "4096",
+    "interpolation_points": "200",
+    "maximum_number_of_scatterings": "100000",
+    "DM_mass": "0.3",
+    "DM_spin": "0.5",
+    "DM_fraction": "1.0",
+    "DM_light": "true",
+    "DM_interaction": '"SI"',
+    "DM_isospin_conserved": "true",
+    "DM_cross_section_nucleon": "1.0e-36",
+    "DM_cross_section_electron": "0.0",
+    "DM_form_factor": '"Contact"',
+    "DM_distribution": '"SHM"',
+    "DM_local_density": "0.4",
+    "SHM_v0": "220.0",
+    "SHM_vEscape": "544.0",
+    "SHM_vObserver": "[11.1, 232.2, 7.3]",
+}
+
+
+def write_config(path, **over):
+    keys = dict(BASE)
+    keys.update(over)
+    with open(path, "w") as f:
+        f.write("// run configuration written by the test\n")
+        for k, v in keys.items():
+            if v is not None:
+                f.write("%s = %s;\n" % (k, v))
+    return path
+
+
+def run(cfg, cwd, timeout=600):
+    return subprocess.run([DMS_SUN, cfg], cwd=cwd, capture_output=True, text=True, timeout=timeout)
+
+
+needs_cli = pytest.mark.skipif(not os.path.exists(DMS_SUN), reason="dms_sun not built (run __graft_entry__.build())")
+
+
+@needs_cli
+def test_usage_without_arguments():
+    p = subprocess.run([DMS_SUN], capture_output=True, text=True, timeout=60)
+    assert p.returncode == 1 and "Usage" in p.stderr
+
+
+@needs_cli
+@pytest.mark.parametrize("over, message", [
+    ({"run_mode": '"Parameter scan"'}, "is not provided by this engine"),
+    ({"run_mode": '"Spectrum"'}, "Run mode Spectrum not recognized."),
+    ({"interpolation_points": "-1"}, "'interpolation_points' must be non-negative."),
+    ({"sample_size": None}, "No 'sample_size' setting in configuration file."),
+    ({"DM_interaction": '"SD"'}, "is not provided by this engine (SI contact is)."),
+    ({"DM_light": "false"}, "DM_light = false"),
+    ({"maximum_number_of_scatterings": "1.5"}, "'maximum_number_of_scatterings' must be a non-negative integer."),
+])
+def test_configuration_errors(tmp_path, over, message):
+    p = run(write_config(tmp_path / "bad.cfg", **over), tmp_path, timeout=60)
+    assert p.returncode != 0
+    assert message in p.stderr, p.stderr
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_parameter_point_run_writes_reference_outputs(tmp_path):
+    p = run(write_config(tmp_path / "point.cfg"), tmp_path)
+    assert p.returncode == 0, p.stderr
+    for label in ("Simulation data summary", "Simulated trajectories:", "Average # of scatterings:", "Capture rate raw error",
+                  "Simulation time"):
+        assert label in p.stdout, p.stdout
+    dirs = [d for d in os.listdir(tmp_path) if d.startswith("results_")]
+    assert len(dirs) == 1
+    out = tmp_path / dirs[0]
+    head, rows = {}, []
+    for line in open(out / "bincount.txt"):
+        if line.startswith("#"):
+            if "=" in line:
+                k, v = line[1:].split("=", 1)
+                head[k.strip()] = v.strip()
+        elif line.strip():
+            rows.append(line.split())
+    for key in ("captured_particles", "valid_trajectories", "capture_rate_valid", "capture_rate_valid_err",
+                "capture_rate_valid_CI_95_lower", "capture_rate_valid_CI_95_upper", "numerical_failure_rate",
+                "average_scatterings"):
+        assert key in head, key
+    assert int(head["captured_particles"]) >= 16
+    assert len(rows) == 2000 and all(len(r) == 9 for r in rows)
+    assert sum(float(r[1]) for r in rows) > 0.0
+    ev = [l.split() for l in open(out / "evaporation_times.txt") if l.strip() and not l.startswith("#")]
+    assert "# format_version = 3" in open(out / "evaporation_times.txt").read()
+    assert all(len(r) == 3 and float(r[2]) > 0.0 for r in ev)
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_capture_run_prints_capture_summary(tmp_path):
+    p = run(write_config(tmp_path / "capture.cfg", run_mode='"Capture"', sample_size="64", max_trajectories="8192",
+                         DM_mass="1.0", DM_cross_section_nucleon="1.0e-35"), tmp_path)
+    assert p.returncode == 0, p.stderr
+    for label in ("CAPTURE MODE summary", "Simulated trajectories:", "Total # of scatterings:", "Captured particle rate [1/s]:"):
+        assert label in p.stdout, p.stdout
+    assert not [d for d in os.listdir(tmp_path) if d.startswith("results_")]

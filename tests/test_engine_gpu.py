@@ -122,3 +122,29 @@ def test_errors_leave_context_usable(engine, replay):
         engine.run([(pid, 0, 10 ** 7)], dms_b200.run_opts(seed=5, time_limit_s=0.05))
     out = engine.run_records(pid, 0, 4, dms_b200.run_opts(seed=7, time_limit_s=60.0))
     assert all(out["records"][i].termination_reason in range(11) for i in range(4))
+
+
+def test_direct_rate_point_matches_oracle(engine, oracle):
+    """interpolation_points = 0 builds no grid: every lookup sums the 64 channels on the fly
+    (src/Solar_Model.cpp:397-405, 324-342).  The device uses CUDA's erf/exp and the oracle the C
+    library's, so rates agree to 1e-13 relative, not bit for bit; replayed Capture-mode
+    trajectories then agree in outcome and, where the outcome agrees, to 1e-8 relative."""
+    pid = engine.add_point(dms_b200.point_params(0.3, 1e-36, interpolation_points=0))
+    oracle.set_point(oracle_point_params(0.3, 1e-36, interpolation_points=0))
+    with pytest.raises(dms_b200.EngineError):
+        engine.rate_grid(pid, 2)
+    rng = np.random.default_rng(5)
+    r = rng.uniform(0, RSUN_KM, 200)
+    v = rng.uniform(0, 3000, 200)
+    got = engine.rate(pid, r, v, interpolated=True)
+    want = np.array([oracle.query(5, a, b) for a, b in zip(r, v)])
+    assert np.max(np.abs(got - want) / np.maximum(np.abs(want), 1e-300)) < 1e-13
+    n = 64
+    opts = dms_b200.run_opts(seed=7, capture_mode=True, max_scatterings=10 ** 5, time_limit_s=120.0)
+    a = engine.run_records(pid, 0, n, opts)["records"]
+    b = oracle.run_records(7, pid, 0, n, capture_mode=True, max_scatterings=10 ** 5)["records"]
+    same = [i for i in range(n) if outcome(a[i]) == outcome(b[i])]
+    assert len(same) >= 0.9 * n, [(i, outcome(a[i]), outcome(b[i])) for i in range(n) if i not in same][:5]
+    for i in same:
+        x, y = np.array(state(a[i])), np.array(state(b[i]))
+        assert np.max(np.abs(x - y) / np.maximum(np.abs(y), 1e-300)) < 1e-8

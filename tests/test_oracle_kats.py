@@ -139,3 +139,14 @@ int main(void){
     assert out[0] == "6627e8d5 e169c58d bc57ac4c 9b00dbd8"
     assert out[1] == "408f276d 41c83b0e a20bc7c6 6d5451fd"
     assert out[2] == "d16cfe09 94fdcceb 5001e420 24126ea1"
+
+
+def test_direct_rate_point_uses_the_computed_rate(oracle):
+    """interpolation_points < 2 builds no grid: every lookup is the 64-channel sum
+    (Interpolate_Total_DM_Scattering_Rate with N < 2, src/Solar_Model.cpp:397-405)."""
+    import dms_ctypes
+    oracle.set_point(dms_ctypes.point_params(0.3, 1e-36, interpolation_points=0))
+    for r, v in ((1.0e4, 300.0), (3.0e5, 900.0), (6.9e5, 1500.0)):
+        assert oracle.query(5, r, v) == oracle.query(6, r, v) > 0.0
+    recs = oracle.run_records(7, 0, 0, 8, capture_mode=True, max_scatterings=10 ** 5)["records"]
+    assert all(recs[i].termination_reason in range(11) for i in range(8))
