@@ -584,7 +584,10 @@ enum RkResult : int
 	RK_FORCED = 2,
 };
 
-__device__ __forceinline__ int rk45_attempt(const DevSolar& S, Prop& p, int inner)
+// The same attempt with the six stages written out: a longer instruction stream (more
+// instruction-cache pressure with many warps) but a shorter dependent chain for a lane that
+// runs alone.
+__device__ __forceinline__ int rk45_attempt_unrolled(const DevSolar& S, Prop& p, int inner)
 {
 	{
 		const double dt = p.time_step;
@@ -618,6 +621,78 @@ __device__ __forceinline__ int rk45_attempt(const DevSolar& S, Prop& p, int inne
 		const double r5 = p.radius + 16.0 / 135.0 * kr0 + 6656.0 / 12825.0 * kr2 + 28561.0 / 56430.0 * kr3 - 9.0 / 50.0 * kr4 + 2.0 / 55.0 * kr5;
 		const double v5 = p.v_radial + 16.0 / 135.0 * kv0 + 6656.0 / 12825.0 * kv2 + 28561.0 / 56430.0 * kv3 - 9.0 / 50.0 * kv4 + 2.0 / 55.0 * kv5;
 		const double p5 = p.phi + 16.0 / 135.0 * kp0 + 6656.0 / 12825.0 * kp2 + 28561.0 / 56430.0 * kp3 - 9.0 / 50.0 * kp4 + 2.0 / 55.0 * kp5;
+		const double e0 = fabs(r5 - r4), e1 = fabs(v5 - v4), e2 = fabs(p5 - p4);
+		const double new_step = next_step_size(dt, e0, e1, e2);
+		const bool within = isfinite(e0) && e0 <= DMS_RK45_TOL_R_KM && isfinite(e1) && e1 <= DMS_RK45_TOL_V_KMS && isfinite(e2) && e2 <= DMS_RK45_TOL_PHI;
+		if(within)
+		{
+			p.time = p.time + dt;
+			p.radius = r4 < 0.0 ? 0.0 : r4;
+			p.v_radial = v4;
+			p.phi = p4;
+			p.time_step = new_step;
+			return RK_ACCEPTED;
+		}
+		if(new_step < DMS_RK45_ABS_MIN_STEP_S || inner >= DMS_RK45_MAX_INNER_RETRIES)
+		{
+			const bool ok = isfinite(r4) && isfinite(v4) && isfinite(p4);
+			p.time = p.time + DMS_RK45_ABS_MIN_STEP_S;
+			if(ok)
+			{
+				p.radius = r4 < 0.0 ? 0.0 : r4;
+				p.v_radial = v4;
+				p.phi = p4;
+			}
+			p.time_step = DMS_RK45_ABS_MIN_STEP_S;
+			return RK_FORCED;
+		}
+		p.time_step = new_step;
+		return RK_RETRY;
+	}
+}
+
+// Runge-Kutta-Fehlberg 4(5) coefficients of src/Simulation_Trajectory.cpp:1492-1540: stage
+// weights a[i][j] (stage i from the slopes of stages j < i) and the 4th / 5th order weights.
+// Zero weights are absent from the reference's sums and are skipped here.
+__constant__ double RKF_A[6][5] = {
+	{0.0, 0.0, 0.0, 0.0, 0.0},
+	{1.0 / 4.0, 0.0, 0.0, 0.0, 0.0},
+	{3.0 / 32.0, 9.0 / 32.0, 0.0, 0.0, 0.0},
+	{1932.0 / 2197.0, -(7200.0 / 2197.0), 7296.0 / 2197.0, 0.0, 0.0},
+	{439.0 / 216.0, -8.0, 3680.0 / 513.0, -(845.0 / 4104.0), 0.0},
+	{-(8.0 / 27.0), 2.0, -(3544.0 / 2565.0), 1859.0 / 4104.0, -(11.0 / 40.0)}};
+__constant__ double RKF_B4[6] = {25.0 / 216.0, 0.0, 1408.0 / 2565.0, 2197.0 / 4104.0, -(1.0 / 5.0), 0.0};
+__constant__ double RKF_B5[6] = {16.0 / 135.0, 0.0, 6656.0 / 12825.0, 28561.0 / 56430.0, -(9.0 / 50.0), 2.0 / 55.0};
+
+__device__ __forceinline__ int rk45_attempt(const DevSolar& S, Prop& p, int inner)
+{
+	{
+		const double dt = p.time_step;
+		const double J = p.J;
+		// The six stages run as one loop.  Every later stage's radius and radial speed, and the
+		// two solutions, are accumulators that start at the step's initial value and receive
+		// a * k as each slope becomes known: the same additions, in the same order, as the
+		// reference's written-out sums (x + (-a) * k equals x - a * k exactly).
+		double R1 = p.radius, R2 = p.radius, R3 = p.radius, R4 = p.radius, R5 = p.radius;
+		double V1 = p.v_radial, V2 = p.v_radial, V3 = p.v_radial, V4 = p.v_radial, V5 = p.v_radial;
+		double r4 = p.radius, v4 = p.v_radial, p4 = p.phi, r5 = p.radius, v5 = p.v_radial, p5 = p.phi;
+#pragma unroll 1
+		for(int j = 0; j < 6; j++)
+		{
+			const double ri = j == 0 ? p.radius : j == 1 ? R1 : j == 2 ? R2 : j == 3 ? R3 : j == 4 ? R4 : R5;
+			const double vi = j == 0 ? p.v_radial : j == 1 ? V1 : j == 2 ? V2 : j == 3 ? V3 : j == 4 ? V4 : V5;
+			const double kr = dt * vi;
+			const double kv = dt * dv_dt(J, ri, solar_gm(S, ri));
+			const double kp = dt * dphi_dt(p, ri);
+			if(j < 1) { const double a = RKF_A[1][j]; R1 = R1 + a * kr; V1 = V1 + a * kv; }
+			if(j < 2) { const double a = RKF_A[2][j]; R2 = R2 + a * kr; V2 = V2 + a * kv; }
+			if(j < 3) { const double a = RKF_A[3][j]; R3 = R3 + a * kr; V3 = V3 + a * kv; }
+			if(j < 4) { const double a = RKF_A[4][j]; R4 = R4 + a * kr; V4 = V4 + a * kv; }
+			if(j < 5) { const double a = RKF_A[5][j]; R5 = R5 + a * kr; V5 = V5 + a * kv; }
+			const double b4 = RKF_B4[j], b5 = RKF_B5[j];
+			if(b4 != 0.0) { r4 = r4 + b4 * kr; v4 = v4 + b4 * kv; p4 = p4 + b4 * kp; }
+			if(b5 != 0.0) { r5 = r5 + b5 * kr; v5 = v5 + b5 * kv; p5 = p5 + b5 * kp; }
+		}
 		const double e0 = fabs(r5 - r4), e1 = fabs(v5 - v4), e2 = fabs(p5 - p4);
 		const double new_step = next_step_size(dt, e0, e1, e2);
 		const bool within = isfinite(e0) && e0 <= DMS_RK45_TOL_R_KM && isfinite(e1) && e1 <= DMS_RK45_TOL_V_KMS && isfinite(e2) && e2 <= DMS_RK45_TOL_PHI;

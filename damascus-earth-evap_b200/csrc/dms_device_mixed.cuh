@@ -87,51 +87,52 @@ __device__ __forceinline__ void stage_rates(const PropF& p, float r, float gm, f
 	dp = (p.radial_mode || p.J == 0.0f || r <= 0.0f) ? 0.0f : p.J * inv2;
 }
 
+// Fehlberg weights in FP32 and the error weights (b5 - b4) in FP64
+__constant__ float RKF_A_F[6][5] = {
+	{0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+	{1.0f / 4.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+	{3.0f / 32.0f, 9.0f / 32.0f, 0.0f, 0.0f, 0.0f},
+	{1932.0f / 2197.0f, -7200.0f / 2197.0f, 7296.0f / 2197.0f, 0.0f, 0.0f},
+	{439.0f / 216.0f, -8.0f, 3680.0f / 513.0f, -845.0f / 4104.0f, 0.0f},
+	{-8.0f / 27.0f, 2.0f, -3544.0f / 2565.0f, 1859.0f / 4104.0f, -11.0f / 40.0f}};
+__constant__ float RKF_B4_F[6] = {25.0f / 216.0f, 0.0f, 1408.0f / 2565.0f, 2197.0f / 4104.0f, -1.0f / 5.0f, 0.0f};
+__constant__ double RKF_E[6] = {16.0 / 135.0 - 25.0 / 216.0, 0.0, 6656.0 / 12825.0 - 1408.0 / 2565.0, 28561.0 / 56430.0 - 2197.0 / 4104.0,
+                                -9.0 / 50.0 + 1.0 / 5.0, 2.0 / 55.0};
+
 // One pass of the Runge_Kutta_45_Step retry loop (src/Simulation_Trajectory.cpp:1492-1600):
 // FP32 stages, FP64 error norm and state update.
 __device__ __forceinline__ int rk45_attempt_f(const DevSolar& S, const DevSolarF& F, PropF& p, int inner)
 {
 	const float dt = static_cast<float>(p.time_step);
 	const float r = static_cast<float>(p.radius), v = static_cast<float>(p.v_radial);
-	float kr0, kr1, kr2, kr3, kr4, kr5, kv0, kv1, kv2, kv3, kv4, kv5, kp0, kp2, kp3, kp4, kp5, ri, a, b;
-	stage_rates(p, r, gm_f(S, F, r), a, b);
-	kr0 = dt * v;
-	kv0 = dt * a;
-	kp0 = dt * b;
-	ri = r + 0.25f * kr0;
-	kr1 = dt * (v + 0.25f * kv0);
-	stage_rates(p, ri, gm_f(S, F, ri), a, b);
-	kv1 = dt * a;  // stage 1's dphi has no weight in either solution
-	ri = r + (3.0f / 32.0f) * kr0 + (9.0f / 32.0f) * kr1;
-	kr2 = dt * (v + (3.0f / 32.0f) * kv0 + (9.0f / 32.0f) * kv1);
-	stage_rates(p, ri, gm_f(S, F, ri), a, b);
-	kv2 = dt * a;
-	kp2 = dt * b;
-	ri = r + (1932.0f / 2197.0f) * kr0 - (7200.0f / 2197.0f) * kr1 + (7296.0f / 2197.0f) * kr2;
-	kr3 = dt * (v + (1932.0f / 2197.0f) * kv0 - (7200.0f / 2197.0f) * kv1 + (7296.0f / 2197.0f) * kv2);
-	stage_rates(p, ri, gm_f(S, F, ri), a, b);
-	kv3 = dt * a;
-	kp3 = dt * b;
-	ri = r + (439.0f / 216.0f) * kr0 - 8.0f * kr1 + (3680.0f / 513.0f) * kr2 - (845.0f / 4104.0f) * kr3;
-	kr4 = dt * (v + (439.0f / 216.0f) * kv0 - 8.0f * kv1 + (3680.0f / 513.0f) * kv2 - (845.0f / 4104.0f) * kv3);
-	stage_rates(p, ri, gm_f(S, F, ri), a, b);
-	kv4 = dt * a;
-	kp4 = dt * b;
-	ri = r - (8.0f / 27.0f) * kr0 + 2.0f * kr1 - (3544.0f / 2565.0f) * kr2 + (1859.0f / 4104.0f) * kr3 - (11.0f / 40.0f) * kr4;
-	kr5 = dt * (v - (8.0f / 27.0f) * kv0 + 2.0f * kv1 - (3544.0f / 2565.0f) * kv2 + (1859.0f / 4104.0f) * kv3 - (11.0f / 40.0f) * kv4);
-	stage_rates(p, ri, gm_f(S, F, ri), a, b);
-	kv5 = dt * a;
-	kp5 = dt * b;
-	// 4th-order increments (FP32) and the 5th - 4th order difference in FP64
-	const float dr4 = (25.0f / 216.0f) * kr0 + (1408.0f / 2565.0f) * kr2 + (2197.0f / 4104.0f) * kr3 - 0.2f * kr4;
-	const float dv4 = (25.0f / 216.0f) * kv0 + (1408.0f / 2565.0f) * kv2 + (2197.0f / 4104.0f) * kv3 - 0.2f * kv4;
-	const float dp4 = (25.0f / 216.0f) * kp0 + (1408.0f / 2565.0f) * kp2 + (2197.0f / 4104.0f) * kp3 - 0.2f * kp4;
-	// (b5 - b4): 16/135 - 25/216, 0, 6656/12825 - 1408/2565, 28561/56430 - 2197/4104, -9/50 + 1/5, 2/55
-	const double c0 = 16.0 / 135.0 - 25.0 / 216.0, c2 = 6656.0 / 12825.0 - 1408.0 / 2565.0, c3 = 28561.0 / 56430.0 - 2197.0 / 4104.0,
-	             c4 = -9.0 / 50.0 + 1.0 / 5.0, c5 = 2.0 / 55.0;
-	const double e0 = fabs(c0 * kr0 + c2 * kr2 + c3 * kr3 + c4 * kr4 + c5 * kr5);
-	const double e1 = fabs(c0 * kv0 + c2 * kv2 + c3 * kv3 + c4 * kv4 + c5 * kv5);
-	const double e2 = fabs(c0 * kp0 + c2 * kp2 + c3 * kp3 + c4 * kp4 + c5 * kp5);
+	// stages as one loop with accumulators for the later stages (see rk45_attempt); the
+	// 4th-order increments in FP32, the (b5 - b4) error sums in FP64
+	float R1 = r, R2 = r, R3 = r, R4 = r, R5 = r, V1 = v, V2 = v, V3 = v, V4 = v, V5 = v;
+	float dr4 = 0.0f, dv4 = 0.0f, dp4 = 0.0f;
+	double er = 0.0, ev = 0.0, ep = 0.0;
+#pragma unroll 1
+	for(int j = 0; j < 6; j++)
+	{
+		const float ri = j == 0 ? r : j == 1 ? R1 : j == 2 ? R2 : j == 3 ? R3 : j == 4 ? R4 : R5;
+		const float vi = j == 0 ? v : j == 1 ? V1 : j == 2 ? V2 : j == 3 ? V3 : j == 4 ? V4 : V5;
+		float a, b;
+		stage_rates(p, ri, gm_f(S, F, ri), a, b);
+		const float kr = dt * vi, kv = dt * a, kp = dt * b;
+		if(j < 1) { const float c = RKF_A_F[1][j]; R1 += c * kr; V1 += c * kv; }
+		if(j < 2) { const float c = RKF_A_F[2][j]; R2 += c * kr; V2 += c * kv; }
+		if(j < 3) { const float c = RKF_A_F[3][j]; R3 += c * kr; V3 += c * kv; }
+		if(j < 4) { const float c = RKF_A_F[4][j]; R4 += c * kr; V4 += c * kv; }
+		if(j < 5) { const float c = RKF_A_F[5][j]; R5 += c * kr; V5 += c * kv; }
+		const float b4 = RKF_B4_F[j];
+		dr4 += b4 * kr;
+		dv4 += b4 * kv;
+		dp4 += b4 * kp;
+		const double c = RKF_E[j];
+		er += c * static_cast<double>(kr);
+		ev += c * static_cast<double>(kv);
+		ep += c * static_cast<double>(kp);
+	}
+	const double e0 = fabs(er), e1 = fabs(ev), e2 = fabs(ep);
 	const bool finite_state = isfinite(dr4) && isfinite(dv4) && isfinite(dp4);
 	// RK45_Next_Step_Size, src/Simulation_Trajectory.cpp:477-502
 	double new_step;

@@ -119,7 +119,11 @@ __device__ __forceinline__ int free_step(const RunParams& R, const DevPoint* __r
 		L.rk_inner = 0;
 	}
 	L.rk_inner++;
+#if DMS_RK_UNROLLED
+	const int rk = rk45_attempt_unrolled(S, L.pr, L.rk_inner);
+#else
 	const int rk = rk45_attempt(S, L.pr, L.rk_inner);
+#endif
 	if(rk == RK_RETRY)
 		return PH_STEP;
 	L.in_rk = 0;
@@ -160,25 +164,42 @@ __device__ __forceinline__ int free_step(const RunParams& R, const DevPoint* __r
 		double dtau = 0.0, tau2 = 0.0;
 		if(s1 > s0 && actual_dt > 0.0)
 		{
-#pragma unroll
-			for(int i = 0; i <= DMS_MAX_OPTICAL_DEPTH_PIECES; i++)
+			// One loop over the piece boundaries (one copy of the rate lookup); the trapezoid
+			// sums are formed as the rates arrive, in the reference's order.  The arrays keep
+			// the boundaries for the scattering-point search, which is rare.
+			double fr_prev = 0.0, rt_prev = 0.0, fr_0 = 0.0, rt_0 = 0.0, fr_2 = 0.0, rt_2 = 0.0, tau2_a = 0.0;
+#pragma unroll 1
+			for(int i = 0; i <= pieces; i++)
 			{
-				if(i > pieces)
-					break;
-				fr[i] = s0 + static_cast<double>(i) / static_cast<double>(pieces) * span;
-				rt[i] = (i == 0 && use_cached) ? rate_before : rate_at_fraction(S, P, before, after, fr[i]);
-				if(!isfinite(rt[i]) || rt[i] < 0.0)
+				const double f = s0 + static_cast<double>(i) / static_cast<double>(pieces) * span;
+				const double rate = (i == 0 && use_cached) ? rate_before : rate_at_fraction(S, P, before, after, f);
+				fr[i] = f;
+				rt[i] = rate;
+				if(!isfinite(rate) || rate < 0.0)
 					invalid = true;
-			}
-			if(!invalid)
-			{
+				if(i > 0 && f > fr_prev)
+					dtau += 0.5 * (rt_prev + rate) * (actual_dt * (f - fr_prev));
 				if(pieces >= 4)
-					tau2 = 0.5 * (rt[0] + rt[2]) * (actual_dt * (fr[2] - fr[0])) + 0.5 * (rt[2] + rt[4]) * (actual_dt * (fr[4] - fr[2]));
-				else
-					for(int i = 0; i < pieces; i++) tau2 += 0.5 * (rt[i] + rt[i + 1]) * (actual_dt * (fr[i + 1] - fr[i]));
-				for(int i = 0; i < pieces; i++)
-					if(fr[i + 1] > fr[i])
-						dtau += 0.5 * (rt[i] + rt[i + 1]) * (actual_dt * (fr[i + 1] - fr[i]));
+				{
+					// two-piece estimate over [0, 2] and [2, 4]
+					if(i == 0)
+					{
+						fr_0 = f;
+						rt_0 = rate;
+					}
+					else if(i == 2)
+					{
+						fr_2 = f;
+						rt_2 = rate;
+						tau2_a = 0.5 * (rt_0 + rt_2) * (actual_dt * (fr_2 - fr_0));
+					}
+					else if(i == 4)
+						tau2 = tau2_a + 0.5 * (rt_2 + rate) * (actual_dt * (f - fr_2));
+				}
+				else if(i > 0)
+					tau2 += 0.5 * (rt_prev + rate) * (actual_dt * (f - fr_prev));
+				fr_prev = f;
+				rt_prev = rate;
 			}
 		}
 		if(invalid || !isfinite(dtau) || dtau < 0.0)

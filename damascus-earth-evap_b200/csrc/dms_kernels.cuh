@@ -10,6 +10,10 @@
 #ifndef DMS_TRAJ_MIN_BLOCKS
 #define DMS_TRAJ_MIN_BLOCKS 4
 #endif
+// RK45 form of the FP64 kernel: 1 = stages written out, 0 = one loop over the stages
+#ifndef DMS_RK_UNROLLED
+#define DMS_RK_UNROLLED 1
+#endif
 #ifndef DMS_TRAJ_MIN_BLOCKS_MIXED
 #define DMS_TRAJ_MIN_BLOCKS_MIXED 4
 #endif

@@ -167,25 +167,39 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 		float dtau_f = 0.0f, tau2 = 0.0f;  // optical depths of one step (<= 0.1) in FP32
 		if(s1 > s0 && actual_dt > 0.0)
 		{
-#pragma unroll
-			for(int i = 0; i <= DMS_MAX_OPTICAL_DEPTH_PIECES; i++)
+			// one loop over the piece boundaries, trapezoids formed as the rates arrive
+			float fr_prev = 0.0f, rt_prev = 0.0f, fr_0 = 0.0f, rt_0 = 0.0f, fr_2 = 0.0f, rt_2 = 0.0f, tau2_a = 0.0f;
+#pragma unroll 1
+			for(int i = 0; i <= pieces; i++)
 			{
-				if(i > pieces)
-					break;
-				fr[i] = s0 + static_cast<float>(i) / static_cast<float>(pieces) * span;
-				rt[i] = (i == 0 && use_cached) ? static_cast<float>(rate_before) : rate_at_fraction_f(S, P, grid, before, after, fr[i]);
-				if(!isfinite(rt[i]) || rt[i] < 0.0f)
+				const float f = s0 + static_cast<float>(i) / static_cast<float>(pieces) * span;
+				const float rate = (i == 0 && use_cached) ? static_cast<float>(rate_before) : rate_at_fraction_f(S, P, grid, before, after, f);
+				fr[i] = f;
+				rt[i] = rate;
+				if(!isfinite(rate) || rate < 0.0f)
 					invalid = true;
-			}
-			if(!invalid)
-			{
+				if(i > 0 && f > fr_prev)
+					dtau_f += 0.5f * (rt_prev + rate) * (adt * (f - fr_prev));
 				if(pieces >= 4)
-					tau2 = 0.5f * (rt[0] + rt[2]) * (adt * (fr[2] - fr[0])) + 0.5f * (rt[2] + rt[4]) * (adt * (fr[4] - fr[2]));
-				else
-					for(int i = 0; i < pieces; i++) tau2 += 0.5f * (rt[i] + rt[i + 1]) * (adt * (fr[i + 1] - fr[i]));
-				for(int i = 0; i < pieces; i++)
-					if(fr[i + 1] > fr[i])
-						dtau_f += 0.5f * (rt[i] + rt[i + 1]) * (adt * (fr[i + 1] - fr[i]));
+				{
+					if(i == 0)
+					{
+						fr_0 = f;
+						rt_0 = rate;
+					}
+					else if(i == 2)
+					{
+						fr_2 = f;
+						rt_2 = rate;
+						tau2_a = 0.5f * (rt_0 + rt_2) * (adt * (fr_2 - fr_0));
+					}
+					else if(i == 4)
+						tau2 = tau2_a + 0.5f * (rt_2 + rate) * (adt * (f - fr_2));
+				}
+				else if(i > 0)
+					tau2 += 0.5f * (rt_prev + rate) * (adt * (f - fr_prev));
+				fr_prev = f;
+				rt_prev = rate;
 			}
 		}
 		const double dtau = static_cast<double>(dtau_f);

@@ -620,16 +620,16 @@ __device__ __forceinline__ int finish_scatter(const RunParams& R, const DevPoint
 }
 
 #ifndef DMS_SCATTER_BATCH
-#define DMS_SCATTER_BATCH 8
+#define DMS_SCATTER_BATCH 16
 #endif
 #ifndef DMS_SCATTER_MAX_WAIT
-#define DMS_SCATTER_MAX_WAIT 16
+#define DMS_SCATTER_MAX_WAIT 32
 #endif
 #ifndef DMS_FINAL_BATCH
-#define DMS_FINAL_BATCH 1
+#define DMS_FINAL_BATCH 8
 #endif
 #ifndef DMS_FINAL_MAX_WAIT
-#define DMS_FINAL_MAX_WAIT 16
+#define DMS_FINAL_MAX_WAIT 32
 #endif
 
 template <class Lane, class Step>

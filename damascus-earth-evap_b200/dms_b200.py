@@ -9,7 +9,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIBRARY = os.path.join(HERE, "libdms_cuda.so")
+# the in-tree engine library; DMS_LIBRARY names another build of it
+LIBRARY = os.environ.get("DMS_LIBRARY", os.path.join(HERE, "libdms_cuda.so"))
 SOLAR_MODEL = os.path.join(HERE, "data", "model_agss09.dat")
 
 NUM_BINS = 2000
