@@ -439,6 +439,40 @@ def run_grid(args):
     engine.close()
 
 
+def run_stress(args):
+    """The heavy-scattering point (m = 0.1 GeV, sigma_n = 1e-33 cm^2, max 1e7 scatterings, seed
+    11): mean free paths far below R_sun and up to millions of scatterings per captured
+    particle.  Its full run (262144 captures) is far beyond a bench; each form runs a
+    2^20-trajectory launch for a bounded wall time and reports its scattering rate (finished
+    and unfinished trajectories) and, among finished trajectories, the fraction cut off by the
+    scattering limit."""
+    import dms_b200
+    engine = dms_b200.Engine(0)
+    pid = engine.add_point(dms_b200.point_params(0.1, 1e-33, interpolation_points=GRID_N))
+    out = {"workload": "m=0.1 GeV sigma_n=1e-33 cm2, max 1e7 scatterings, seed 11, 2^20 trajectories, "
+                       "bounded to %.0f s per form" % args.stress_seconds}
+    for name, prec in (("fp64", dms_b200.PRECISION_FP64), ("mixed", dms_b200.PRECISION_MIXED)):
+        engine.reset_results(pid)
+        opts = dms_b200.run_opts(seed=11, max_scatterings=10 ** 7, time_limit_s=args.stress_seconds, precision=prec)
+        try:
+            engine.run([(pid, 0, 1 << 20)], opts)
+        except dms_b200.EngineError as e:
+            if "cancelled" not in str(e):
+                raise
+        ms = engine.last_kernel_ms()
+        c = engine.results(pid, events_capacity=1)["counters"]
+        finished = c["trajectories"]
+        out[name] = {"kernel_ms": ms,
+                     "scatterings_per_s": (c["total_scatterings"] + c["unfinished_scatterings"]) / ms * 1e3,
+                     "steps_per_s": (c["rk_steps"] + c["unfinished_rk_steps"]) / ms * 1e3,
+                     "finished_trajectories": finished, "unfinished_trajectories": c["unfinished_trajectories"],
+                     "captured": c["captured"],
+                     "cutoff_fraction_of_finished": c["reasons"][5] / finished if finished else None}
+    out["mixed_over_fp64_scatterings_per_s"] = out["mixed"]["scatterings_per_s"] / out["fp64"]["scatterings_per_s"]
+    print(json.dumps(out), flush=True)
+    engine.close()
+
+
 def run_profile_case(args):
     """One trajectory launch for a profiler (no timing): `single` runs trajectory id 1612 alone
     (the longest of ids 0..16383 of this point, 38944 accepted steps in the FP64 form: the
@@ -485,9 +519,13 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64", help="form used by --profile-case")
     ap.add_argument("--grid-seconds", type=float, default=0.0,
                     help="run the 20-point grid launch for this many seconds per form instead of the bench")
+    ap.add_argument("--stress-seconds", type=float, default=0.0,
+                    help="run the heavy-scattering point for this many seconds per form instead of the bench")
     args = ap.parse_args()
     if args.grid_seconds > 0:
         run_grid(args)
+    elif args.stress_seconds > 0:
+        run_stress(args)
     elif args.profile_case:
         run_profile_case(args)
     elif args.impl == "reference":
