@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <iostream>
 #include <mutex>
 #include <new>
 #include <string>
@@ -21,6 +22,7 @@
 #include <vector>
 
 #include "../../include/dms.h"
+#include "../../include/dms_driver.h"
 #include "dms_host_model.h"
 #include "dms_kernels.cuh"
 
@@ -50,6 +52,8 @@ struct dms_ctx
 	double* d_hists = nullptr;
 	dms_evaporation_event* d_events = nullptr;
 	unsigned long long* d_event_count = nullptr;
+	dms_reflection* d_refl = nullptr;              // [points x event capacity]
+	unsigned long long* d_refl_count = nullptr;
 	uint64_t event_capacity = 1ULL << 20;
 	// run scratch
 	double2* d_lane_hist = nullptr;
@@ -94,11 +98,16 @@ int Grow_Points(dms_ctx* ctx, int needed)
 	double* nh = nullptr;
 	dms_evaporation_event* ne = nullptr;
 	unsigned long long* nn = nullptr;
+	dms_reflection* nr = nullptr;
+	unsigned long long* nrc = nullptr;
 	DMS_CUDA(ctx, cudaMalloc(&np, sizeof(DevPoint) * cap));
 	DMS_CUDA(ctx, cudaMalloc(&nc, sizeof(unsigned long long) * DMS_NUM_COUNTERS * cap));
 	DMS_CUDA(ctx, cudaMalloc(&nh, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS * cap));
 	DMS_CUDA(ctx, cudaMalloc(&ne, sizeof(dms_evaporation_event) * ctx->event_capacity * cap));
 	DMS_CUDA(ctx, cudaMalloc(&nn, sizeof(unsigned long long) * cap));
+	DMS_CUDA(ctx, cudaMalloc(&nr, sizeof(dms_reflection) * ctx->event_capacity * cap));
+	DMS_CUDA(ctx, cudaMalloc(&nrc, sizeof(unsigned long long) * cap));
+	DMS_CUDA(ctx, cudaMemset(nrc, 0, sizeof(unsigned long long) * cap));
 	DMS_CUDA(ctx, cudaMemset(nc, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS * cap));
 	DMS_CUDA(ctx, cudaMemset(nh, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS * cap));
 	DMS_CUDA(ctx, cudaMemset(nn, 0, sizeof(unsigned long long) * cap));
@@ -112,12 +121,20 @@ int Grow_Points(dms_ctx* ctx, int needed)
 			DMS_CUDA(ctx, cudaMemcpy(ne + p * ctx->event_capacity, ctx->d_events + p * ctx->event_capacity,
 			                         sizeof(dms_evaporation_event) * ctx->event_capacity, cudaMemcpyDeviceToDevice));
 		DMS_CUDA(ctx, cudaMemcpy(nn, ctx->d_event_count, sizeof(unsigned long long) * old, cudaMemcpyDeviceToDevice));
+		for(int p = 0; p < old; p++)
+			DMS_CUDA(ctx, cudaMemcpy(nr + p * ctx->event_capacity, ctx->d_refl + p * ctx->event_capacity,
+			                         sizeof(dms_reflection) * ctx->event_capacity, cudaMemcpyDeviceToDevice));
+		DMS_CUDA(ctx, cudaMemcpy(nrc, ctx->d_refl_count, sizeof(unsigned long long) * old, cudaMemcpyDeviceToDevice));
 	}
 	cudaFree(ctx->d_points);
 	cudaFree(ctx->d_counters);
 	cudaFree(ctx->d_hists);
 	cudaFree(ctx->d_events);
 	cudaFree(ctx->d_event_count);
+	cudaFree(ctx->d_refl);
+	cudaFree(ctx->d_refl_count);
+	ctx->d_refl = nr;
+	ctx->d_refl_count = nrc;
 	ctx->d_points = np;
 	ctx->d_counters = nc;
 	ctx->d_hists = nh;
@@ -336,6 +353,8 @@ void dms_destroy(dms_ctx* ctx)
 	cudaFree(ctx->d_hists);
 	cudaFree(ctx->d_events);
 	cudaFree(ctx->d_event_count);
+	cudaFree(ctx->d_refl);
+	cudaFree(ctx->d_refl_count);
 	cudaFree(ctx->d_lane_hist);
 	cudaFree(ctx->d_queue);
 	cudaFree(ctx->d_status);
@@ -549,6 +568,7 @@ int dms_add_point(dms_ctx* ctx, const dms_point_params* params, int* point_id)
 	DMS_CUDA(ctx, cudaMemset(ctx->d_counters + static_cast<size_t>(id) * DMS_NUM_COUNTERS, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_hists + static_cast<size_t>(id) * DMS_NUM_HISTS * DMS_NUM_BINS, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_event_count + id, 0, sizeof(unsigned long long)));
+	DMS_CUDA(ctx, cudaMemset(ctx->d_refl_count + id, 0, sizeof(unsigned long long)));
 	if(point_id)
 		*point_id = id;
 	return DMS_OK;
@@ -674,6 +694,8 @@ int dms_run(dms_ctx* ctx, const dms_run_opts* opts, const dms_work_range* ranges
 	p.events = ctx->d_events;
 	p.event_count = ctx->d_event_count;
 	p.event_capacity = ctx->event_capacity;
+	p.reflections = ctx->d_refl;
+	p.reflection_count = ctx->d_refl_count;
 	rc = Launch_And_Wait(ctx, opts, p);
 	cudaFree(d);
 	return rc;
@@ -727,6 +749,8 @@ int dms_run_records(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64
 	p.events = ctx->d_events;
 	p.event_count = ctx->d_event_count;
 	p.event_capacity = ctx->event_capacity;
+	p.reflections = ctx->d_refl;
+	p.reflection_count = ctx->d_refl_count;
 	rc = Launch_And_Wait(ctx, opts, p);
 	if(rc == DMS_OK || rc == DMS_ERR_CANCELLED || rc == DMS_ERR_BUDGET)
 	{
@@ -764,6 +788,16 @@ int dms_get_results(dms_ctx* ctx, int point_id, dms_point_results* r)
 			DMS_CUDA(ctx, cudaMemcpy(r->events, ctx->d_events + static_cast<size_t>(point_id) * ctx->event_capacity,
 			                         sizeof(dms_evaporation_event) * n, cudaMemcpyDeviceToHost));
 	}
+	unsigned long long nrefl = 0;
+	DMS_CUDA(ctx, cudaMemcpy(&nrefl, ctx->d_refl_count + point_id, sizeof nrefl, cudaMemcpyDeviceToHost));
+	r->reflections_count = std::min<uint64_t>(nrefl, ctx->event_capacity);
+	if(r->reflections && r->reflections_capacity > 0)
+	{
+		const uint64_t n = std::min<uint64_t>(r->reflections_count, r->reflections_capacity);
+		if(n > 0)
+			DMS_CUDA(ctx, cudaMemcpy(r->reflections, ctx->d_refl + static_cast<size_t>(point_id) * ctx->event_capacity,
+			                         sizeof(dms_reflection) * n, cudaMemcpyDeviceToHost));
+	}
 	return DMS_OK;
 }
 
@@ -777,6 +811,7 @@ int dms_reset_results(dms_ctx* ctx, int point_id)
 	DMS_CUDA(ctx, cudaMemset(ctx->d_counters + static_cast<size_t>(point_id) * DMS_NUM_COUNTERS, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_hists + static_cast<size_t>(point_id) * DMS_NUM_HISTS * DMS_NUM_BINS, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_event_count + point_id, 0, sizeof(unsigned long long)));
+	DMS_CUDA(ctx, cudaMemset(ctx->d_refl_count + point_id, 0, sizeof(unsigned long long)));
 	return DMS_OK;
 }
 
@@ -908,6 +943,8 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 	p.events = ctx->d_events;
 	p.event_count = ctx->d_event_count;
 	p.event_capacity = ctx->event_capacity;
+	p.reflections = ctx->d_refl;
+	p.reflection_count = ctx->d_refl_count;
 	p.records = d_records;
 	p.rec_hist_dt = d_hist_dt;
 	p.rec_hist_v2dt = d_hist_v2dt;
@@ -951,6 +988,164 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 		return Fail(ctx, DMS_ERR_BUDGET, "run stopped: per-lane iteration budget exhausted");
 	if(status & STATUS_IC_REJECTION)
 		ctx->error = "warning: an initial-condition rejection loop hit its attempt bound";
+	return DMS_OK;
+}
+
+}	// extern "C"
+
+// ---- reflection spectrum -----------------------------------------------------------------
+namespace
+{
+// Isoreflection_Ring_Angles (src/Simulation_Utilities.cpp:323-336): upper angles of n
+// equal-area rings around the Sun's velocity
+std::vector<double> Ring_Angles(uint32_t rings)
+{
+	std::vector<double> a;
+	double theta = 0.0;
+	for(uint32_t i = 0; i + 1 < rings; i++)
+	{
+		theta = std::acos(std::cos(theta) - 2.0 / rings);
+		a.push_back(theta);
+	}
+	a.push_back(DMS_PI);
+	return a;
+}
+
+// Speeds of the recorded reflected particles of one ring
+int Ring_Speeds(dms_ctx* ctx, int point_id, uint32_t rings, uint32_t ring, std::vector<double>& speeds, uint64_t& trajectories)
+{
+	if(rings == 0 || ring >= rings)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "isoreflection ring out of range");
+	dms_point_results res;
+	std::memset(&res, 0, sizeof res);
+	int rc = dms_get_results(ctx, point_id, &res);
+	if(rc != DMS_OK)
+		return rc;
+	std::vector<dms_reflection> all(res.reflections_count);
+	res.reflections = all.data();
+	res.reflections_capacity = all.size();
+	rc = dms_get_results(ctx, point_id, &res);
+	if(rc != DMS_OK)
+		return rc;
+	trajectories = res.counters[DMS_CNT_TRAJECTORIES];
+	const std::vector<double> angles = Ring_Angles(rings);
+	speeds.clear();
+	for(const dms_reflection& r : all)
+	{
+		uint32_t k = 0;
+		if(rings > 1)
+		{
+			const double c = r.cos_sun_velocity < -1.0 ? -1.0 : (r.cos_sun_velocity > 1.0 ? 1.0 : r.cos_sun_velocity);
+			const double theta = std::acos(c);
+			while(k + 1 < rings && theta > angles[k]) k++;
+		}
+		if(k == ring)
+			speeds.push_back(r.speed_kms);
+	}
+	return DMS_OK;
+}
+}	// namespace
+
+extern "C" {
+
+int dms_get_reflection_spectrum(dms_ctx* ctx, int point_id, uint32_t rings, uint32_t ring, double dm_density_gev_cm3,
+                                dms_reflection_spectrum* out)
+{
+	if(!ctx || !out)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
+		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	std::vector<double> speeds;
+	uint64_t trajectories = 0;
+	const int rc = Ring_Speeds(ctx, point_id, rings, ring, speeds, trajectories);
+	if(rc != DMS_OK)
+		return rc;
+	const PointConstants& c = ctx->points[point_id];
+	std::memset(out, 0, sizeof *out);
+	out->trajectories = trajectories;
+	out->reflections = speeds.size();
+	out->reflection_ratio = trajectories > 0 ? static_cast<double>(speeds.size()) / trajectories : 0.0;
+	// DM_Entering_Rate, src/Reflection_Spectrum.cpp:63-71: number density in 1/km^3, R_sun in km
+	const double n_dm = dm_density_gev_cm3 / c.m_dm * 1.0e15;
+	const double vesc2 = ctx->tables.vesc2.back();  // v_esc^2 at R_sun
+	out->entering_rate_per_s = DMS_RSUN_KM * DMS_RSUN_KM * DMS_PI * n_dm * (c.avg_speed + vesc2 * c.eta0);
+	out->reflection_rate_per_s = out->reflection_ratio * out->entering_rate_per_s;
+	out->distance_au = 1.0;
+	const double d_cm = DMS_AU_KM * 1.0e5;
+	out->flux_per_s_cm2 = out->reflection_rate_per_s / (4.0 * DMS_PI * d_cm * d_cm) * rings;
+	double vmax = 0.0, sum = 0.0;
+	for(double v : speeds)
+	{
+		vmax = std::max(vmax, v);
+		sum += v;
+	}
+	out->speed_min_kms = 0.0;  // 0.75 x the minimum speed threshold u_min = 0 of the run modes
+	out->speed_max_kms = 1.05 * vmax;
+	out->mean_speed_kms = speeds.empty() ? 0.0 : sum / speeds.size();
+	return DMS_OK;
+}
+
+int dms_reflection_spectrum_pdf(dms_ctx* ctx, int point_id, uint32_t rings, uint32_t ring, const double* u_kms, size_t n, double* pdf)
+{
+	if(!ctx || (n > 0 && (!u_kms || !pdf)))
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
+		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	std::vector<double> speeds;
+	uint64_t trajectories = 0;
+	const int rc = Ring_Speeds(ctx, point_id, rings, ring, speeds, trajectories);
+	if(rc != DMS_OK)
+		return rc;
+	const size_t m = speeds.size();
+	if(m < 2)
+	{
+		for(size_t i = 0; i < n; i++) pdf[i] = 0.0;
+		return DMS_OK;
+	}
+	std::sort(speeds.begin(), speeds.end());
+	double mean = 0.0, var = 0.0, vmax = speeds.back();
+	for(double v : speeds) mean += v;
+	mean /= m;
+	for(double v : speeds) var += (v - mean) * (v - mean);
+	const double sigma = std::sqrt(var / (m - 1));
+	const double iqr = speeds[(3 * m) / 4] - speeds[m / 4];
+	const double spread = iqr > 0.0 ? std::min(sigma, iqr / 1.34) : sigma;
+	const double h = 0.9 * spread * std::pow(static_cast<double>(m), -0.2);
+	const double lo = 0.0, hi = 1.05 * vmax;
+	const double norm = 1.0 / (m * h * std::sqrt(2.0 * DMS_PI));
+	for(size_t i = 0; i < n; i++)
+	{
+		const double u = u_kms[i];
+		if(!(u >= lo && u <= hi) || !(h > 0.0))
+		{
+			pdf[i] = 0.0;
+			continue;
+		}
+		double s = 0.0;
+		for(double v : speeds)
+		{
+			const double a = (u - v) / h, b = (u + v - 2.0 * lo) / h;  // kernel and its mirror at lo
+			s += std::exp(-0.5 * a * a) + std::exp(-0.5 * b * b);
+		}
+		pdf[i] = s * norm;
+	}
+	return DMS_OK;
+}
+
+int dms_print_reflection_summary(const dms_reflection_spectrum* s)
+{
+	if(!s)
+		return DMS_ERR_INVALID_ARGUMENT;
+	// Reflection_Spectrum::Print_Summary, src/Reflection_Spectrum.cpp:47-59
+	const char* sep = "\n----------------------------------------\n";
+	std::cout << sep << "Reflection spectrum" << std::endl
+	          << "\tSpeed domain [km/sec]:\t\t\t[" << s->speed_min_kms << ", " << s->speed_max_kms << "]" << std::endl
+	          << "\tReflected particles:\t\t\t" << s->reflections << " of " << s->trajectories << std::endl
+	          << "\tMean speed at 1 AU [km/sec]:\t\t" << s->mean_speed_kms << std::endl
+	          << "\tTotal DM entering rate [1/s]:\t\t" << s->entering_rate_per_s << std::endl
+	          << "\tTotal reflection rate [1/s]:\t\t" << s->reflection_rate_per_s << std::endl
+	          << "\tDistance from Sun [AU]:\t\t\t" << s->distance_au << std::endl
+	          << "\tTotal reflection flux [1/s/cm^2]:\t" << s->flux_per_s_cm2 << sep;
 	return DMS_OK;
 }
 

@@ -78,6 +78,8 @@ struct RunParams
 	dms_evaporation_event* events;  // n_points x event_capacity
 	unsigned long long* event_count;// n_points
 	uint64_t event_capacity;
+	dms_reflection* reflections;    // n_points x event_capacity
+	unsigned long long* reflection_count; // n_points
 	// records mode (records != nullptr): one record per work index
 	dms_traj_record* records;
 	double* rec_hist_dt;

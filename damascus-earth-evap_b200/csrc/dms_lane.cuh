@@ -305,7 +305,28 @@ __device__ __noinline__ void finalize(const RunParams& R, const DevPoint* __rest
 					flags |= DMS_REC_REFLECTED;
 					Event fin = L.cur;
 					if(hyperbolic_kepler_shift(fin, DMS_AU_KM))
+					{
 						flags |= DMS_REC_REFLECT_SHIFT_OK;
+						if(R.records == nullptr && R.reflections != nullptr)
+						{
+							// the reflection-spectrum sample, src/Data_Generation.cpp:829-840
+							const double speed = ev_speed(fin);
+							const double* vs = P->vel_obs;
+							const double sun = sqrt(vs[0] * vs[0] + vs[1] * vs[1] + vs[2] * vs[2]);
+							const double cosine = (fin.x.x * vs[0] + fin.x.y * vs[1] + fin.x.z * vs[2]) / ev_radius(fin) / sun;
+							const unsigned long long k = atomicAdd(R.reflection_count + L.point, 1ULL);
+							if(k < R.event_capacity)
+							{
+								dms_reflection rf;
+								rf.trajectory_id = L.D.traj + 1;
+								rf.speed_kms = speed;
+								rf.cos_sun_velocity = cosine;
+								R.reflections[static_cast<size_t>(L.point) * R.event_capacity + k] = rf;
+							}
+							else
+								atomicAdd(R.counters + static_cast<size_t>(L.point) * DMS_NUM_COUNTERS + DMS_CNT_REFLECTIONS_DROPPED, 1ULL);
+						}
+					}
 				}
 			}
 		}

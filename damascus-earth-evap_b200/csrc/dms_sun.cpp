@@ -102,6 +102,11 @@ int main(int argc, char* argv[])
 		                        std::to_string(std::log10(cfg.sigma_nucleon_cm2)) + "/";
 		if(dms_write_outputs(ctx, pid, &s, cfg.DM_mass_gev, cfg.sigma_nucleon_cm2, out.c_str()) != DMS_OK)
 			std::cerr << "Warning: failed to write the output files into " << out << std::endl;
+		// reflection spectrum, src/main.cpp:95-99
+		dms_reflection_spectrum spectrum;
+		if(cfg.isoreflection_rings == 1 && dms_get_reflection_spectrum(ctx, pid, 1, 0, cfg.rho_local, &spectrum) == DMS_OK &&
+		   spectrum.reflections > 0)
+			dms_print_reflection_summary(&spectrum);
 	}
 	dms_destroy(ctx);
 	const double total = std::chrono::duration<double>(std::chrono::system_clock::now() - start).count();

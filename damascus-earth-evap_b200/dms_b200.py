@@ -21,7 +21,7 @@ COUNTER_NAMES = {0: "trajectories", 1: "free", 2: "reflected", 3: "captured", 4:
                  9: "final_reflection_shift_failures", 10: "numerical_failures", 11: "computational_truncations",
                  12: "total_scatterings", 13: "rk_steps", 14: "events_dropped", 15: "rk_attempts",
                  27: "unfinished_trajectories", 28: "unfinished_scatterings", 29: "unfinished_rk_steps",
-                 30: "unfinished_rk_attempts"}
+                 30: "unfinished_rk_attempts", 31: "reflections_dropped"}
 REASON_BASE = 16
 HIST_NAMES = ["captured_dt", "captured_v2dt", "not_captured_dt", "not_captured_v2dt", "captured_dt_sq",
               "captured_v2dt_sq", "not_captured_dt_sq", "not_captured_v2dt_sq"]
@@ -66,10 +66,22 @@ class EvaporationEvent(ctypes.Structure):
     _fields_ = [("trajectory_id", ctypes.c_uint64), ("lifetime_unbinding", ctypes.c_double)]
 
 
+class Reflection(ctypes.Structure):
+    _fields_ = [("trajectory_id", ctypes.c_uint64), ("speed_kms", ctypes.c_double), ("cos_sun_velocity", ctypes.c_double)]
+
+
 class PointResults(ctypes.Structure):
     _fields_ = [("counters", ctypes.c_uint64 * NUM_COUNTERS), ("histograms", ctypes.POINTER(ctypes.c_double)),
                 ("events", ctypes.POINTER(EvaporationEvent)), ("events_capacity", ctypes.c_uint64),
-                ("events_count", ctypes.c_uint64)]
+                ("events_count", ctypes.c_uint64), ("reflections", ctypes.POINTER(Reflection)),
+                ("reflections_capacity", ctypes.c_uint64), ("reflections_count", ctypes.c_uint64)]
+
+
+class ReflectionSpectrum(ctypes.Structure):
+    _fields_ = [("trajectories", ctypes.c_uint64), ("reflections", ctypes.c_uint64), ("reflection_ratio", ctypes.c_double),
+                ("entering_rate_per_s", ctypes.c_double), ("reflection_rate_per_s", ctypes.c_double),
+                ("distance_au", ctypes.c_double), ("flux_per_s_cm2", ctypes.c_double), ("speed_min_kms", ctypes.c_double),
+                ("speed_max_kms", ctypes.c_double), ("mean_speed_kms", ctypes.c_double)]
 
 
 def point_params(mass_gev, sigma_p_cm2, sigma_e_cm2=1e-80, interpolation_points=1000, v0=220.0, vesc=544.0,
@@ -113,6 +125,8 @@ def library():
     lib.dms_num_bins.restype = c.c_int
     lib.dms_last_kernel_ms.argtypes = [vp, c.POINTER(c.c_double)]
     lib.dms_measure_fp64_peak.argtypes = [vp, c.POINTER(c.c_double)]
+    lib.dms_get_reflection_spectrum.argtypes = [vp, c.c_int, c.c_uint32, c.c_uint32, c.c_double, c.POINTER(ReflectionSpectrum)]
+    lib.dms_reflection_spectrum_pdf.argtypes = [vp, c.c_int, c.c_uint32, c.c_uint32, vp, c.c_size_t, vp]
     _lib = lib
     return lib
 
@@ -221,20 +235,39 @@ class Engine:
             out["hist_dt"], out["hist_v2dt"] = hd, hv
         return out
 
-    def results(self, point, events_capacity=1 << 20):
+    def results(self, point, events_capacity=1 << 20, reflections_capacity=0):
         res = PointResults()
         hist = np.zeros(NUM_HISTS * NUM_BINS)
         events = (EvaporationEvent * events_capacity)()
+        refl = np.zeros(reflections_capacity, dtype=[("trajectory_id", np.uint64), ("speed_kms", np.float64),
+                                                      ("cos_sun_velocity", np.float64)])
         res.histograms = hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         res.events = events
         res.events_capacity = events_capacity
+        res.reflections = refl.ctypes.data_as(ctypes.POINTER(Reflection))
+        res.reflections_capacity = reflections_capacity
         self._check(self.lib.dms_get_results(self.h, point, ctypes.byref(res)))
         counters = {name: int(res.counters[k]) for k, name in COUNTER_NAMES.items()}
         counters["reasons"] = [int(res.counters[REASON_BASE + k]) for k in range(11)]
         n = min(res.events_count, events_capacity)
         ev = np.array([(events[i].trajectory_id, events[i].lifetime_unbinding) for i in range(n)],
                       dtype=[("trajectory_id", np.uint64), ("lifetime_unbinding", np.float64)])
-        return {"counters": counters, "histograms": hist.reshape(NUM_HISTS, NUM_BINS), "events": ev}
+        out = {"counters": counters, "histograms": hist.reshape(NUM_HISTS, NUM_BINS), "events": ev,
+               "reflections_count": int(res.reflections_count)}
+        if reflections_capacity:
+            out["reflections"] = refl[:min(res.reflections_count, reflections_capacity)]
+        return out
+
+    def reflection_spectrum(self, point, rings=1, ring=0, dm_density_gev_cm3=0.4):
+        s = ReflectionSpectrum()
+        self._check(self.lib.dms_get_reflection_spectrum(self.h, point, rings, ring, dm_density_gev_cm3, ctypes.byref(s)))
+        return {name: getattr(s, name) for name, _ in ReflectionSpectrum._fields_}
+
+    def reflection_pdf(self, point, u_kms, rings=1, ring=0):
+        u = np.ascontiguousarray(u_kms, dtype=np.float64)
+        out = np.zeros_like(u)
+        self._check(self.lib.dms_reflection_spectrum_pdf(self.h, point, rings, ring, u.ctypes.data, u.size, out.ctypes.data))
+        return out
 
     def last_kernel_ms(self):
         ms = ctypes.c_double(0.0)

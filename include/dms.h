@@ -241,6 +241,7 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 #define DMS_CNT_UNFINISHED_SCATTERINGS    28
 #define DMS_CNT_UNFINISHED_RK_STEPS       29
 #define DMS_CNT_UNFINISHED_RK_ATTEMPTS    30
+#define DMS_CNT_REFLECTIONS_DROPPED       31   /* reflected-particle records beyond the buffer capacity */
 #define DMS_NUM_COUNTERS                  32
 
 /* Histogram slots (each DMS_NUM_BINS doubles), src/Data_Generation.cpp:101-110 */
@@ -261,6 +262,18 @@ typedef struct
 	double lifetime_unbinding;
 } dms_evaporation_event;
 
+/* A reflected particle (not captured, escaped outward after at least one scattering) whose
+ * orbit was carried to 1 AU (Hyperbolic_Kepler_Shift): the data behind the reflection
+ * spectrum, src/Data_Generation.cpp:824-846.  cos_sun_velocity is the cosine of the angle
+ * between its position at 1 AU and the Sun's velocity (Isoreflection_Angle,
+ * src/Simulation_Utilities.cpp:82-92), from which the isoreflection ring follows. */
+typedef struct
+{
+	uint64_t trajectory_id;            /* trajectory index + 1 */
+	double speed_kms;                  /* speed at 1 AU */
+	double cos_sun_velocity;
+} dms_reflection;
+
 typedef struct
 {
 	uint64_t counters[DMS_NUM_COUNTERS];
@@ -268,6 +281,9 @@ typedef struct
 	dms_evaporation_event* events;     /* caller buffer of events_capacity entries, or NULL */
 	uint64_t events_capacity;
 	uint64_t events_count;             /* events stored on the device (copied: min(count, capacity)) */
+	dms_reflection* reflections;       /* caller buffer of reflections_capacity entries, or NULL */
+	uint64_t reflections_capacity;
+	uint64_t reflections_count;        /* reflections stored on the device */
 } dms_point_results;
 
 int dms_get_results(dms_ctx* ctx, int point_id, dms_point_results* results);

@@ -62,6 +62,34 @@ int dms_write_outputs(dms_ctx* ctx, int point_id, const dms_generate_summary* su
                       const char* output_dir);
 int dms_print_summary(dms_ctx* ctx, int point_id, const dms_generate_summary* summary, int capture_mode);
 
+/* ---- reflection spectrum (Reflection_Spectrum, src/Reflection_Spectrum.cpp:12-73) -------------
+ * From the reflected particles recorded by dms_run (dms_reflection): the particles of one
+ * isoreflection ring (equal-area rings around the Sun's velocity, Isoreflection_Ring_Angles,
+ * src/Simulation_Utilities.cpp:323-336), the DM entering rate pi R_sun^2 n (<u> + v_esc^2 <1/u>)
+ * (DM_Entering_Rate, :63-71), the reflection rate (entering rate x reflected fraction) and the
+ * flux at 1 AU. */
+typedef struct
+{
+	uint64_t trajectories;             /* trajectories behind the sample */
+	uint64_t reflections;              /* recorded reflected particles in the ring */
+	double reflection_ratio;           /* reflections / trajectories (Reflection_Ratio) */
+	double entering_rate_per_s;
+	double reflection_rate_per_s;
+	double distance_au;                /* 1 */
+	double flux_per_s_cm2;             /* reflection rate / (4 pi d^2) x rings */
+	double speed_min_kms, speed_max_kms;  /* spectrum domain: [0, 1.05 x highest speed] */
+	double mean_speed_kms;
+} dms_reflection_spectrum;
+
+int dms_get_reflection_spectrum(dms_ctx* ctx, int point_id, uint32_t rings, uint32_t ring, double dm_density_gev_cm3,
+                                dms_reflection_spectrum* out);
+/* Speed distribution of the ring's reflected particles at the n speeds u_kms [1/(km/s)]: a
+ * Gaussian kernel density estimate (Silverman bandwidth, mirrored at the lower domain edge),
+ * zero outside the domain.  Multiply by reflection_rate_per_s for the differential spectrum. */
+int dms_reflection_spectrum_pdf(dms_ctx* ctx, int point_id, uint32_t rings, uint32_t ring, const double* u_kms, size_t n,
+                                double* pdf);
+int dms_print_reflection_summary(const dms_reflection_spectrum* spectrum);
+
 #ifdef __cplusplus
 }
 #endif

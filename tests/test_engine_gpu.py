@@ -148,3 +148,28 @@ def test_direct_rate_point_matches_oracle(engine, oracle):
     for i in same:
         x, y = np.array(state(a[i])), np.array(state(b[i]))
         assert np.max(np.abs(x - y) / np.maximum(np.abs(y), 1e-300)) < 1e-8
+
+
+def test_reflected_particles_recorded(engine):
+    """Reflected particles carried to 1 AU are recorded with their speed (the reflection-spectrum
+    sample, src/Data_Generation.cpp:824-846); their number equals the reflected count minus the
+    failed final Kepler shifts, and the spectrum's rates follow from it."""
+    pid = engine.add_point(dms_b200.point_params(0.3, 1e-36, interpolation_points=1000))
+    n = 1 << 14
+    engine.run([(pid, 0, n)], dms_b200.run_opts(seed=7, max_scatterings=10 ** 6, time_limit_s=300.0))
+    res = engine.results(pid, events_capacity=1, reflections_capacity=1 << 16)
+    c = res["counters"]
+    refl = res["reflections"]
+    assert len(refl) == c["reflected"] - c["final_reflection_shift_failures"] > 0
+    assert np.all(refl["speed_kms"] > 0.0) and np.all(np.abs(refl["cos_sun_velocity"]) <= 1.0)
+    assert len(set(refl["trajectory_id"].tolist())) == len(refl)
+    s = engine.reflection_spectrum(pid, rings=1, ring=0, dm_density_gev_cm3=0.4)
+    assert s["reflections"] == len(refl) and s["trajectories"] == n
+    assert s["reflection_rate_per_s"] == pytest.approx(s["entering_rate_per_s"] * len(refl) / n, rel=1e-12)
+    assert s["speed_max_kms"] == pytest.approx(1.05 * refl["speed_kms"].max(), rel=1e-12)
+    # equal-area rings split the sample
+    parts = [engine.reflection_spectrum(pid, rings=4, ring=k)["reflections"] for k in range(4)]
+    assert sum(parts) == len(refl)
+    u = np.linspace(0.0, s["speed_max_kms"], 2001)
+    pdf = engine.reflection_pdf(pid, u)
+    assert np.all(pdf >= 0.0) and abs(np.trapezoid(pdf, u) - 1.0) < 0.05
