@@ -294,23 +294,29 @@ def run_engine_arm(args):
     barrier()
     e2e_s = time.perf_counter() - t0
     # steady state: a queue far longer than the run, stopped by the wall-clock limit; every
-    # scattering done counts, in finished and in unfinished trajectories
+    # scattering done counts, in finished and in unfinished trajectories.  Two windows of
+    # different length are run and the rate is the difference quotient, which removes the
+    # initial-state pre-pass and the ramp-up and ramp-down of the lanes.
     steady = {}
     if args.steady_seconds > 0:
-        for name, prec in (("fp64", fp64), ("mixed", mixed)):
+        def window(prec, seconds):
             engine.reset_results(solo)
-            o = dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT,
-                                  time_limit_s=args.steady_seconds, precision=prec)
+            o = dms_b200.run_opts(seed=SEED, capture_mode=False, max_scatterings=MAX_SCAT, time_limit_s=seconds,
+                                  precision=prec)
             try:
-                engine.run([(solo, 1 << 40, 1 << 21)], o)
+                engine.run([(solo, 1 << 40, 1 << 23)], o)
             except dms_b200.EngineError as e:
                 if "cancelled" not in str(e):
                     raise
-            ms = engine.last_kernel_ms()
             c = engine.results(solo, events_capacity=1)["counters"]
-            steady[name] = {"scatterings_per_s": (c["total_scatterings"] + c["unfinished_scatterings"]) / ms * 1e3,
-                            "steps_per_s": (c["rk_steps"] + c["unfinished_rk_steps"]) / ms * 1e3,
-                            "kernel_ms": ms}
+            return (engine.last_kernel_ms(), c["total_scatterings"] + c["unfinished_scatterings"],
+                    c["rk_steps"] + c["unfinished_rk_steps"])
+        for name, prec in (("fp64", fp64), ("mixed", mixed)):
+            t1, s1, n1 = window(prec, 0.5 * args.steady_seconds)
+            t2, s2, n2 = window(prec, 1.5 * args.steady_seconds)
+            dt = (t2 - t1) * 1e-3
+            steady[name] = {"scatterings_per_s": (s2 - s1) / dt, "steps_per_s": (n2 - n1) / dt,
+                            "windows_ms": [t1, t2]}
         steady["mixed_over_fp64"] = steady["mixed"]["scatterings_per_s"] / steady["fp64"]["scatterings_per_s"]
 
     c = tot["counters"]
