@@ -66,6 +66,14 @@ struct dms_ctx
 	int* d_cancel = nullptr;
 	cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 	double last_kernel_ms = 0.0;
+	// progress of the launch in flight (dms_set_progress_callback, dms_peek_*)
+	dms_progress_fn progress_fn = nullptr;
+	void* progress_user = nullptr;
+	double progress_interval_s = 1.0;
+	cudaStream_t peek_stream = nullptr;  // non-blocking: its copies run beside the kernel
+	bool running = false;
+	uint64_t launch_total = 0;
+	std::chrono::steady_clock::time_point launch_start{};
 };
 
 namespace
@@ -111,6 +119,8 @@ int Grow_Points(dms_ctx* ctx, int needed)
 	DMS_CUDA(ctx, cudaMemset(nc, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS * cap));
 	DMS_CUDA(ctx, cudaMemset(nh, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS * cap));
 	DMS_CUDA(ctx, cudaMemset(nn, 0, sizeof(unsigned long long) * cap));
+	// an evaporation slot with trajectory id 0 is unpublished (dms_peek_results)
+	DMS_CUDA(ctx, cudaMemset(ne, 0, sizeof(dms_evaporation_event) * ctx->event_capacity * cap));
 	const int old = static_cast<int>(ctx->points.size());
 	if(old > 0)
 	{
@@ -249,32 +259,51 @@ int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 	DMS_CUDA(ctx, cudaGetLastError());
 	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
 	const auto start = std::chrono::steady_clock::now();
-	bool cancelled_by_limit = false;
+	ctx->running = true;
+	ctx->launch_total = p.total;
+	ctx->launch_start = start;
+	auto last_progress = start;
+	bool cancelled_by_limit = false, cancelled_by_hook = false;
 	for(;;)
 	{
 		const cudaError_t q = cudaStreamQuery(ctx->stream);
 		if(q == cudaSuccess)
 			break;
 		if(q != cudaErrorNotReady)
+		{
+			ctx->running = false;
 			return Fail(ctx, DMS_ERR_CUDA, std::string("trajectory kernel: ") + cudaGetErrorString(q));
+		}
+		const auto now = std::chrono::steady_clock::now();
 		if(o->time_limit_s > 0.0 && !cancelled_by_limit)
 		{
-			const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+			const double el = std::chrono::duration<double>(now - start).count();
 			if(el > o->time_limit_s)
 			{
 				*reinterpret_cast<volatile int*>(ctx->h_cancel) = 1;
 				cancelled_by_limit = true;
 			}
 		}
+		if(ctx->progress_fn && std::chrono::duration<double>(now - last_progress).count() >= ctx->progress_interval_s)
+		{
+			last_progress = now;
+			if(ctx->progress_fn(ctx, ctx->progress_user) != 0 && !cancelled_by_hook)
+			{
+				*reinterpret_cast<volatile int*>(ctx->h_cancel) = 1;
+				cancelled_by_hook = true;
+			}
+		}
 		std::this_thread::sleep_for(std::chrono::microseconds(200));
 	}
+	ctx->running = false;
 	float kernel_ms = 0.0f;
 	DMS_CUDA(ctx, cudaEventElapsedTime(&kernel_ms, ctx->ev_start, ctx->ev_stop));
 	ctx->last_kernel_ms = kernel_ms;
 	unsigned int status = 0;
 	DMS_CUDA(ctx, cudaMemcpy(&status, ctx->d_status, sizeof status, cudaMemcpyDeviceToHost));
 	if(status & STATUS_CANCELLED)
-		return Fail(ctx, DMS_ERR_CANCELLED, cancelled_by_limit ? "run cancelled: wall-clock limit reached" : "run cancelled");
+		return Fail(ctx, DMS_ERR_CANCELLED, cancelled_by_limit ? "run cancelled: wall-clock limit reached"
+		                                    : cancelled_by_hook ? "run cancelled by the progress callback" : "run cancelled");
 	if(status & STATUS_BUDGET)
 		return Fail(ctx, DMS_ERR_BUDGET, "run stopped: per-lane iteration budget exhausted");
 	if(status & STATUS_IC_REJECTION)
@@ -323,6 +352,7 @@ int dms_create(dms_ctx** out, int device)
 	ctx->device = device;
 	if(cudaSetDevice(device) != cudaSuccess || cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
 	   cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+	   cudaStreamCreateWithFlags(&ctx->peek_stream, cudaStreamNonBlocking) != cudaSuccess ||
 	   cudaMalloc(&ctx->d_queue, sizeof(unsigned long long)) != cudaSuccess || cudaMalloc(&ctx->d_status, sizeof(unsigned int)) != cudaSuccess ||
 	   cudaHostAlloc(&ctx->h_cancel, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
 	   cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->d_cancel), ctx->h_cancel, 0) != cudaSuccess ||
@@ -366,6 +396,8 @@ void dms_destroy(dms_ctx* ctx)
 		cudaEventDestroy(ctx->ev_stop);
 	if(ctx->stream)
 		cudaStreamDestroy(ctx->stream);
+	if(ctx->peek_stream)
+		cudaStreamDestroy(ctx->peek_stream);
 	delete ctx;
 }
 
@@ -812,6 +844,71 @@ int dms_reset_results(dms_ctx* ctx, int point_id)
 	DMS_CUDA(ctx, cudaMemset(ctx->d_hists + static_cast<size_t>(point_id) * DMS_NUM_HISTS * DMS_NUM_BINS, 0, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_event_count + point_id, 0, sizeof(unsigned long long)));
 	DMS_CUDA(ctx, cudaMemset(ctx->d_refl_count + point_id, 0, sizeof(unsigned long long)));
+	DMS_CUDA(ctx, cudaMemset(ctx->d_events + static_cast<size_t>(point_id) * ctx->event_capacity, 0,
+	                         sizeof(dms_evaporation_event) * ctx->event_capacity));
+	return DMS_OK;
+}
+
+int dms_set_progress_callback(dms_ctx* ctx, dms_progress_fn fn, void* user, double interval_s)
+{
+	if(!ctx)
+		return DMS_ERR_INVALID_ARGUMENT;
+	if(fn && !(interval_s >= 0.0 && interval_s < 1e9))
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "progress interval must be finite and non-negative");
+	ctx->progress_fn = fn;
+	ctx->progress_user = fn ? user : nullptr;
+	ctx->progress_interval_s = fn ? interval_s : 1.0;
+	return DMS_OK;
+}
+
+int dms_peek_progress(dms_ctx* ctx, dms_progress* out)
+{
+	if(!ctx || !out)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	std::memset(out, 0, sizeof *out);
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	unsigned long long head = 0;
+	DMS_CUDA(ctx, cudaMemcpyAsync(&head, ctx->d_queue, sizeof head, cudaMemcpyDeviceToHost, ctx->peek_stream));
+	DMS_CUDA(ctx, cudaStreamSynchronize(ctx->peek_stream));
+	out->running = ctx->running ? 1 : 0;
+	out->total = ctx->launch_total;
+	out->dispatched = std::min<uint64_t>(head, ctx->launch_total);
+	out->elapsed_s = ctx->running ? std::chrono::duration<double>(std::chrono::steady_clock::now() - ctx->launch_start).count() : 0.0;
+	return DMS_OK;
+}
+
+int dms_peek_results(dms_ctx* ctx, int point_id, dms_point_results* r)
+{
+	if(!ctx || !r)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
+		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	cudaStream_t s = ctx->peek_stream;
+	unsigned long long count = 0;
+	DMS_CUDA(ctx, cudaMemcpyAsync(r->counters, ctx->d_counters + static_cast<size_t>(point_id) * DMS_NUM_COUNTERS,
+	                              sizeof(unsigned long long) * DMS_NUM_COUNTERS, cudaMemcpyDeviceToHost, s));
+	if(r->histograms)
+		DMS_CUDA(ctx, cudaMemcpyAsync(r->histograms, ctx->d_hists + static_cast<size_t>(point_id) * DMS_NUM_HISTS * DMS_NUM_BINS,
+		                              sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS, cudaMemcpyDeviceToHost, s));
+	DMS_CUDA(ctx, cudaMemcpyAsync(&count, ctx->d_event_count + point_id, sizeof count, cudaMemcpyDeviceToHost, s));
+	DMS_CUDA(ctx, cudaStreamSynchronize(s));
+	r->events_count = std::min<uint64_t>(count, ctx->event_capacity);
+	r->reflections_count = 0;
+	if(r->events && r->events_capacity > 0)
+	{
+		const uint64_t n = std::min<uint64_t>(r->events_count, r->events_capacity);
+		if(n > 0)
+		{
+			DMS_CUDA(ctx, cudaMemcpyAsync(r->events, ctx->d_events + static_cast<size_t>(point_id) * ctx->event_capacity,
+			                              sizeof(dms_evaporation_event) * n, cudaMemcpyDeviceToHost, s));
+			DMS_CUDA(ctx, cudaStreamSynchronize(s));
+		}
+		uint64_t k = 0;
+		while(k < n && r->events[k].trajectory_id != 0)
+			k++;
+		r->events_count = k;
+	}
 	return DMS_OK;
 }
 

@@ -290,14 +290,15 @@ std::string Load_Run_Config(const std::string& path, RunConfig& cfg)
 			return "Error in Configuration::Import_Parameter_Scan_Parameter(): 'maximum_number_of_scatterings' must be a non-negative integer.";
 		cfg.maximum_number_of_scatterings = static_cast<uint64_t>(x);
 	}
-	bool snapshot = false;
-	k.Bool("snapshot_enabled", snapshot);
-	if(snapshot && k.Has("snapshot_interval"))
+	// snapshot settings, src/Parameter_Scan.cpp:310-340
+	k.Bool("snapshot_enabled", cfg.snapshot_enabled);
+	if(cfg.snapshot_enabled && k.Has("snapshot_interval"))
 	{
 		if(!k.Number("snapshot_interval", x))
 			return "Error in Configuration::Import_Parameter_Scan_Parameter(): 'snapshot_interval' must be a numeric value.";
-		if(!std::isfinite(x) || x <= 0.0 || std::floor(x) != x)
+		if(!std::isfinite(x) || x < 1.0 || x > 2147483647.0 || std::floor(x) != x)
 			return "Error in Configuration::Import_Parameter_Scan_Parameter(): 'snapshot_interval' must be a positive integer number of seconds.";
+		cfg.snapshot_interval = x;
 	}
 	if(k.Number("max_trajectory_wall_time_sec", x))
 	{

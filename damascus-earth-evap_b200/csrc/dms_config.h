@@ -45,6 +45,8 @@ struct RunConfig
 	uint32_t isoreflection_rings = 1;
 	uint64_t maximum_number_of_scatterings = 100000000000000ULL;
 	double max_trajectory_wall_time_sec = 0.0;
+	bool snapshot_enabled = false;
+	double snapshot_interval = 60.0;  // seconds; the reference's default when snapshots are on
 	std::string output_dir = "./";
 	// DM particle (SI contact, low-mass mode)
 	double DM_mass_gev = 0.0;

@@ -17,8 +17,10 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <memory>
 #include <sstream>
 #include <string>
+#include <dirent.h>
 #include <sys/stat.h>
 #include <unistd.h>
 #include <vector>
@@ -152,6 +154,295 @@ double Numerical_Failure_Ratio(const uint64_t* c)
 {
 	return c[DMS_CNT_TRAJECTORIES] > 0 ? 1.0 * c[DMS_CNT_NUMERICAL_FAILURES] / c[DMS_CNT_TRAJECTORIES] : 0.0;
 }
+
+// The raw capture-rate lines of bincount.txt and of the snapshot reports, with the legacy
+// capture_rate* aliases (src/Data_Generation.cpp:253-278, src/Snapshot_IO.cpp:530-539).
+void Write_Raw_Rate_Lines(std::ostream& f, const Binomial& raw)
+{
+	f << "# capture_rate = " << std::fixed << std::setprecision(8) << raw.rate << "\n";
+	f << "# capture_rate_raw = " << std::fixed << std::setprecision(8) << raw.rate << "\n";
+	f << "# capture_rate_err = " << std::fixed << std::setprecision(8) << raw.err << "\n";
+	f << "# capture_rate_raw_err = " << std::fixed << std::setprecision(8) << raw.err << "\n";
+	f << "# capture_rate_CI_95_lower = " << std::fixed << std::setprecision(8) << raw.lo << "\n";
+	f << "# capture_rate_CI_95_upper = " << std::fixed << std::setprecision(8) << raw.hi << "\n";
+	f << "# capture_rate_raw_CI_95_lower = " << std::fixed << std::setprecision(8) << raw.lo << "\n";
+	f << "# capture_rate_raw_CI_95_upper = " << std::fixed << std::setprecision(8) << raw.hi << "\n";
+}
+
+void Write_Valid_Rate_Lines(std::ostream& f, const Binomial& valid)
+{
+	f << "# capture_rate_valid = " << std::fixed << std::setprecision(8) << valid.rate << "\n";
+	f << "# capture_rate_valid_err = " << std::fixed << std::setprecision(8) << valid.err << "\n";
+	f << "# capture_rate_valid_CI_95_lower = " << std::fixed << std::setprecision(8) << valid.lo << "\n";
+	f << "# capture_rate_valid_CI_95_upper = " << std::fixed << std::setprecision(8) << valid.hi << "\n";
+}
+
+// The 2000 bin rows (sums and sqrt(N var) errors of captured and not-captured samples),
+// src/Data_Generation.cpp:1232-1263 and src/Snapshot_IO.cpp:629-646.
+void Write_Bincount_Rows(std::ostream& f, const double* h, double n_cap, double n_nc)
+{
+	f << "# bin_index  cap_dt[s]  cap_v2dt[km2/s]  cap_err_dt[s]  cap_err_v2dt[km2/s]  not_cap_dt[s]  not_cap_v2dt[km2/s]  not_cap_err_dt[s]  not_cap_err_v2dt[km2/s]\n";
+	for(int b = 0; b < DMS_NUM_BINS; b++)
+	{
+		const double cdt = h[DMS_HIST_CAPTURED_DT * DMS_NUM_BINS + b], cv = h[DMS_HIST_CAPTURED_V2DT * DMS_NUM_BINS + b];
+		const double ndt = h[DMS_HIST_NOT_CAPTURED_DT * DMS_NUM_BINS + b], nv = h[DMS_HIST_NOT_CAPTURED_V2DT * DMS_NUM_BINS + b];
+		f << b << "\t" << std::scientific << std::setprecision(10) << cdt << "\t" << cv << "\t"
+		  << Snapshot_Bin_Error(cdt, h[DMS_HIST_CAPTURED_DT_SQ * DMS_NUM_BINS + b], n_cap) << "\t"
+		  << Snapshot_Bin_Error(cv, h[DMS_HIST_CAPTURED_V2DT_SQ * DMS_NUM_BINS + b], n_cap) << "\t" << ndt << "\t" << nv << "\t"
+		  << Snapshot_Bin_Error(ndt, h[DMS_HIST_NOT_CAPTURED_DT_SQ * DMS_NUM_BINS + b], n_nc) << "\t"
+		  << Snapshot_Bin_Error(nv, h[DMS_HIST_NOT_CAPTURED_V2DT_SQ * DMS_NUM_BINS + b], n_nc) << "\n";
+	}
+}
+
+// Writes a text file through a temporary name and a rename, so a reader never sees a half
+// written report (WriteTextFileAtomically, src/Snapshot_IO.cpp:78-101).
+template <class Body>
+bool Write_Atomically(const std::string& path, Body body)
+{
+	const std::string tmp = path + ".tmp." + std::to_string(getpid());
+	std::ofstream f(tmp, std::ios::out | std::ios::trunc);
+	if(!f.is_open())
+		return false;
+	body(f);
+	f.close();
+	if(!f.good() || std::rename(tmp.c_str(), path.c_str()) != 0)
+	{
+		std::remove(tmp.c_str());
+		return false;
+	}
+	return true;
+}
+
+bool Event_Order(const dms_evaporation_event& a, const dms_evaporation_event& b)
+{
+	if(a.lifetime_unbinding != b.lifetime_unbinding)
+		return a.lifetime_unbinding < b.lifetime_unbinding;
+	return a.trajectory_id < b.trajectory_id;
+}
+
+// Wall-clock progress reports of one Generate_Data call: the reference's heartbeat thread, its
+// per-rank checkpoints and rank 0's merge (src/Snapshot_Heartbeat.cpp:236-354,
+// src/Snapshot_IO.cpp:369-650) collapse into one writer on the thread that drives the launches,
+// called between launches and from the engine's progress hook while a launch is in flight.
+// It reads the device accumulators with dms_peek_results, so nothing is recorded per RK step.
+// Differences, by design: the trajectories in flight (one per lane, tens of thousands) are
+// counted in the rank table but their partial bincounts are not folded into the report (the
+// reference folds the one current trajectory of each rank, src/Snapshot_IO.cpp:424-455), and
+// an evaporation event is assigned to the first report whose read finds it published.
+class Snapshot_Writer
+{
+  public:
+	Snapshot_Writer(dms_ctx* ctx, int point, const dms_generate_opts& g, std::chrono::steady_clock::time_point t0)
+	: ctx_(ctx), point_(point), root_(g.snapshot_dir), interval_(g.snapshot_interval_s), mass_(g.snapshot_mass_gev),
+	  sigma_(g.snapshot_sigma_cm2), t0_(t0), tolerance_(std::max(1.0, 0.1 * g.snapshot_interval_s)),
+	  hist_(DMS_NUM_HISTS * DMS_NUM_BINS)
+	{
+		if(!root_.empty() && root_.back() != '/')
+			root_ += "/";
+		run_id_ = static_cast<uint64_t>(
+			std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::system_clock::now().time_since_epoch()).count());
+		ok_ = Ensure_Directory(root_) && Clear_Previous();
+		if(!ok_)
+			std::cerr << "Warning in Generate_Data(): failed to initialize snapshot directory; snapshots disabled for this run." << std::endl;
+	}
+
+	bool ok() const { return ok_; }
+	void Launch_Begins() { launch_active_ = true; }
+	void Launch_Ends(uint64_t count)
+	{
+		launch_active_ = false;
+		dispatched_before_ += count;
+	}
+
+	// Writes every report whose time has come (a missed-deadline marker for one whose time
+	// passed by more than the tolerance before it could be written).
+	void Tick()
+	{
+		if(!ok_)
+			return;
+		for(double el = Elapsed(); next_ * interval_ <= el; el = Elapsed())
+		{
+			const double target = next_ * interval_;
+			if(el > target + tolerance_ || !Write_Report(next_, launch_active_ ? "running" : "idle_or_waiting", target))
+				Write_Missed(next_, Elapsed());
+			next_++;
+		}
+	}
+
+	// The reports that fall due between the last one and the end of the run, written from the
+	// final state (FinalizeAfterAllRanksDone, src/Snapshot_Heartbeat.cpp:112-170).
+	void Finish(double final_elapsed)
+	{
+		if(!ok_)
+			return;
+		const double last = std::floor(final_elapsed / interval_);
+		for(; next_ <= last; next_++)
+			if(!Write_Report(next_, "done", -1.0))
+				std::cerr << "Warning in Generate_Data(): failed to write snapshot " << Label(next_) << "s." << std::endl;
+	}
+
+  private:
+	long long Label(long long index) const { return index * static_cast<long long>(interval_); }
+	std::string Path(long long index, const char* suffix) const { return root_ + "snapshot_" + std::to_string(Label(index)) + "s" + suffix; }
+	double Elapsed() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count(); }
+
+	bool Clear_Previous()
+	{
+		// only this writer's own files: the reference clears the whole snapshot directory
+		DIR* d = opendir(root_.c_str());
+		if(!d)
+			return false;
+		std::vector<std::string> names;
+		while(dirent* e = readdir(d))
+			if(std::strncmp(e->d_name, "snapshot_", 9) == 0)
+				names.push_back(e->d_name);
+		closedir(d);
+		bool ok = true;
+		for(const auto& n : names)
+			ok = (std::remove((root_ + n).c_str()) == 0) && ok;
+		return ok;
+	}
+
+	// snapshot_status / run id lines common to both files of a report (one rank: always merged)
+	void Write_Status(std::ostream& f) const
+	{
+		f << "# snapshot_status = merged\n";
+		f << "# snapshot_run_id = " << run_id_ << "\n";
+	}
+
+	// deadline_s < 0: the final report, written whatever the time
+	bool Write_Report(long long index, const char* state, double deadline_s)
+	{
+		dms_point_results r;
+		std::memset(&r, 0, sizeof r);
+		if(dms_peek_results(ctx_, point_, &r) != DMS_OK)
+			return false;
+		events_.resize(std::max<uint64_t>(r.events_count, 1) + 1024);
+		std::memset(&r, 0, sizeof r);
+		r.histograms = hist_.data();
+		r.events = events_.data();
+		r.events_capacity = events_.size();
+		dms_progress pr;
+		if(dms_peek_results(ctx_, point_, &r) != DMS_OK || dms_peek_progress(ctx_, &pr) != DMS_OK)
+			return false;
+		const double observed = Elapsed();
+		if(deadline_s >= 0.0 && observed > deadline_s + tolerance_)
+			return false;
+		const uint64_t* c = r.counters;
+		const uint64_t published = std::max<uint64_t>(r.events_count, published_);
+		std::vector<dms_evaporation_event> fresh(events_.begin() + published_, events_.begin() + published);
+		std::sort(fresh.begin(), fresh.end(), Event_Order);
+		const bool done = deadline_s < 0.0;
+		const uint64_t dispatched = dispatched_before_ + (launch_active_ && pr.running ? pr.dispatched : 0);
+		const uint64_t completed = c[DMS_CNT_TRAJECTORIES];
+		const uint64_t in_flight = (!done && dispatched > completed) ? dispatched - completed : 0;
+
+		// WriteSnapshotEvaporationTimeFile, src/Snapshot_IO.cpp:545-576
+		const bool events_ok = Write_Atomically(Path(index, "_evaporation_times.txt"), [&](std::ofstream& f) {
+			Write_Status(f);
+			f << "# snapshot_target_wall_time_s = " << Label(index) << "\n";
+			f << "# snapshot_interval_s = " << std::fixed << std::setprecision(3) << interval_ << "\n";
+			f << "# ready_ranks = 0\n";
+			f << "# missing_ranks = \n";
+			f << "# completed_evaporation_events_assigned_to_snapshot = 1\n";
+			f << "# event_assignment = first published checkpoint after completion\n";
+			f << "# DaMaSCUS-SUN snapshot evaporation times\n";
+			f << "# format_version = 3\n";
+			f << "# DIAGNOSTIC_ONLY = 1\n";
+			f << "# NOT_FOR_FINAL_SURVIVAL_ANALYSIS = 1\n";
+			f << "# completion_time_selected = 1\n";
+			f << "# DM_mass_GeV = " << std::scientific << std::setprecision(6) << mass_ << "\n";
+			f << "# DM_sigma_cm2 = " << std::scientific << std::setprecision(6) << sigma_ << "\n";
+			f << "# sorted_by = lifetime_unbinding_sec rank trajectory_id\n";
+			f << "# rank trajectory_id lifetime_unbinding_sec\n";
+			for(const auto& e : fresh)
+				if(std::isfinite(e.lifetime_unbinding) && e.lifetime_unbinding >= 0.0)
+					f << 0 << "\t" << e.trajectory_id << "\t" << std::scientific << std::setprecision(10) << e.lifetime_unbinding << "\n";
+		});
+		if(!events_ok)
+			return false;
+		published_ = published;
+
+		// WriteSnapshotReportFile + WriteReportHeader, src/Snapshot_IO.cpp:508-543, 578-650
+		return Write_Atomically(Path(index, ".txt"), [&](std::ofstream& f) {
+			const uint64_t valid = Valid(c);
+			Write_Status(f);
+			f << "# Cumulative snapshot report\n";
+			f << "# ready_ranks = 0\n";
+			f << "# missing_ranks = \n";
+			f << "# snapshot_target_wall_time_s = " << Label(index) << "\n";
+			f << "# snapshot_interval_s = " << std::fixed << std::setprecision(3) << interval_ << "\n";
+			f << "# DM_mass_GeV = " << std::scientific << std::setprecision(6) << mass_ << "\n";
+			f << "# DM_sigma_cm2 = " << std::scientific << std::setprecision(6) << sigma_ << "\n";
+			f << "# total_trajectories = " << completed << "\n";
+			f << "# captured_particles = " << c[DMS_CNT_CAPTURED] << "\n";
+			f << "# valid_trajectories = " << valid << "\n";
+			f << "# numerical_failures = " << c[DMS_CNT_NUMERICAL_FAILURES] << "\n";
+			f << "# unresolved_not_captured_trajectories = " << (completed > valid ? completed - valid : 0) << "\n";
+			Write_Raw_Rate_Lines(f, Estimate(completed, c[DMS_CNT_CAPTURED]));
+			Write_Valid_Rate_Lines(f, Estimate(valid, c[DMS_CNT_CAPTURED]));
+			f << "#\n";
+			f << "# [GPU rank status]\n";
+			f << "# rank  state  dispatched_trajectories  in_flight_trajectories  completed_trajectories  completed_scatterings  observed_at_wall_s\n";
+			f << "# 0\t" << state << "\t" << dispatched << "\t" << in_flight << "\t" << completed << "\t" << c[DMS_CNT_TOTAL_SCATTERINGS]
+			  << "\t" << std::scientific << std::setprecision(10) << observed << "\n";
+			f << "#\n";
+			f << "# [Bincount histogram]\n";
+			Write_Bincount_Rows(f, hist_.data(), static_cast<double>(c[DMS_CNT_CAPTURED]), static_cast<double>(c[DMS_CNT_COMPLETED_OUTWARD]));
+		});
+	}
+
+	// WriteMissedSnapshotMarker, src/Snapshot_IO.cpp:925-947
+	void Write_Missed(long long index, double actual_s)
+	{
+		Write_Atomically(Path(index, ".txt"), [&](std::ofstream& f) {
+			f << "# snapshot_status = missed_writer_delay\n";
+			f << "# snapshot_run_id = " << run_id_ << "\n";
+			f << "# snapshot_target_wall_time_s = " << Label(index) << "\n";
+			f << "# snapshot_interval_s = " << std::fixed << std::setprecision(3) << interval_ << "\n";
+			f << "# actual_write_wall_time_s = " << std::fixed << std::setprecision(3) << actual_s << "\n";
+			f << "# note = heartbeat woke too late; no state rewind is available\n";
+		});
+	}
+
+	dms_ctx* ctx_;
+	int point_;
+	std::string root_;
+	double interval_, mass_, sigma_;
+	std::chrono::steady_clock::time_point t0_;
+	double tolerance_;
+	uint64_t run_id_ = 0;
+	bool ok_ = false;
+	bool launch_active_ = false;
+	long long next_ = 1;
+	uint64_t dispatched_before_ = 0;
+	uint64_t published_ = 0;
+	std::vector<double> hist_;
+	std::vector<dms_evaporation_event> events_;
+};
+
+int Snapshot_Hook(dms_ctx*, void* user)
+{
+	static_cast<Snapshot_Writer*>(user)->Tick();
+	return 0;
+}
+
+// Removes the progress hook when the generate call returns, on every path.
+struct Hook_Guard
+{
+	dms_ctx* ctx;
+	~Hook_Guard()
+	{
+		if(ctx)
+			dms_set_progress_callback(ctx, nullptr, nullptr, 0.0);
+	}
+};
+
+bool Snapshot_Interval_Valid(double s)
+{
+	// IsValidSnapshotIntervalSeconds, src/Snapshot_IO.cpp:652-658
+	return std::isfinite(s) && s >= 1.0 && s <= 2147483647.0 && std::floor(s) == s;
+}
 }	// namespace
 
 extern "C" {
@@ -196,8 +487,25 @@ int dms_generate_data(dms_ctx* ctx, int point_id, const dms_generate_opts* g, dm
 	int stop = DMS_STOP_NONE;
 	bool warned = false;
 	const auto t0 = std::chrono::steady_clock::now();
+	std::unique_ptr<Snapshot_Writer> snapshots;
+	Hook_Guard guard{nullptr};
+	if(g->snapshot_dir && !g->capture_mode)
+	{
+		if(!Snapshot_Interval_Valid(g->snapshot_interval_s))
+			return DMS_ERR_INVALID_ARGUMENT;
+		snapshots.reset(new Snapshot_Writer(ctx, point_id, *g, t0));
+		if(snapshots->ok())
+		{
+			rc = dms_set_progress_callback(ctx, Snapshot_Hook, snapshots.get(), std::min(0.1, 0.1 * g->snapshot_interval_s));
+			if(rc != DMS_OK)
+				return rc;
+			guard.ctx = ctx;
+		}
+	}
 	for(;;)
 	{
+		if(snapshots)
+			snapshots->Tick();
 		rc = dms_get_results(ctx, point_id, &res);
 		if(rc != DMS_OK)
 			return rc;
@@ -255,7 +563,11 @@ int dms_generate_data(dms_ctx* ctx, int point_id, const dms_generate_opts* g, dm
 		range.reserved = 0;
 		range.first_trajectory = next_id;
 		range.count = round;
+		if(snapshots)
+			snapshots->Launch_Begins();
 		rc = dms_run(ctx, &opts, &range, 1);
+		if(snapshots)
+			snapshots->Launch_Ends(round);
 		if(rc != DMS_OK)
 			return rc;
 		next_id += round;
@@ -263,6 +575,11 @@ int dms_generate_data(dms_ctx* ctx, int point_id, const dms_generate_opts* g, dm
 		out->final_round_trajectories = round;
 	}
 	out->computing_time_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+	if(snapshots)
+	{
+		dms_set_progress_callback(ctx, nullptr, nullptr, 0.0);
+		snapshots->Finish(out->computing_time_s);
+	}
 	rc = dms_get_results(ctx, point_id, &res);
 	if(rc != DMS_OK)
 		return rc;
@@ -311,14 +628,7 @@ int dms_write_outputs(dms_ctx* ctx, int point_id, const dms_generate_summary* s,
 		f << "# DM_sigma_cm2 = " << std::scientific << std::setprecision(6) << sigma_cm2 << "\n";
 		f << "# total_trajectories = " << N << "\n";
 		f << "# captured_particles = " << c[DMS_CNT_CAPTURED] << "\n";
-		f << "# capture_rate = " << std::fixed << std::setprecision(8) << raw.rate << "\n";
-		f << "# capture_rate_raw = " << std::fixed << std::setprecision(8) << raw.rate << "\n";
-		f << "# capture_rate_err = " << std::fixed << std::setprecision(8) << raw.err << "\n";
-		f << "# capture_rate_raw_err = " << std::fixed << std::setprecision(8) << raw.err << "\n";
-		f << "# capture_rate_CI_95_lower = " << std::fixed << std::setprecision(8) << raw.lo << "\n";
-		f << "# capture_rate_CI_95_upper = " << std::fixed << std::setprecision(8) << raw.hi << "\n";
-		f << "# capture_rate_raw_CI_95_lower = " << std::fixed << std::setprecision(8) << raw.lo << "\n";
-		f << "# capture_rate_raw_CI_95_upper = " << std::fixed << std::setprecision(8) << raw.hi << "\n";
+		Write_Raw_Rate_Lines(f, raw);
 		if(s->early_stop_reason != DMS_STOP_NONE)
 			f << "# EARLY_STOP: " << Stop_Key(s->early_stop_reason) << "\n";
 		f << "# valid_trajectories = " << Valid(c) << "\n";
@@ -337,39 +647,18 @@ int dms_write_outputs(dms_ctx* ctx, int point_id, const dms_generate_summary* s,
 		const double avg = N > 0 ? static_cast<double>(c[DMS_CNT_TOTAL_SCATTERINGS]) / N : 0.0;
 		f << "# average_scatterings = " << std::setprecision(12) << avg << "\n";
 		f << "# simulation_time_seconds = " << std::setprecision(12) << s->computing_time_s << "\n";
-		const Binomial valid = Estimate(Valid(c), c[DMS_CNT_CAPTURED]);
-		f << "# capture_rate_valid = " << std::fixed << std::setprecision(8) << valid.rate << "\n";
-		f << "# capture_rate_valid_err = " << std::fixed << std::setprecision(8) << valid.err << "\n";
-		f << "# capture_rate_valid_CI_95_lower = " << std::fixed << std::setprecision(8) << valid.lo << "\n";
-		f << "# capture_rate_valid_CI_95_upper = " << std::fixed << std::setprecision(8) << valid.hi << "\n";
+		Write_Valid_Rate_Lines(f, Estimate(Valid(c), c[DMS_CNT_CAPTURED]));
 		f << "# numerical_failure_rate = " << std::fixed << std::setprecision(8) << Numerical_Failure_Ratio(c) << "\n";
 		f << "# not_captured_bincount_samples = " << c[DMS_CNT_COMPLETED_OUTWARD] << "\n";
 		if(unresolved > 0)
 			f << "# excluded_incomplete_not_captured = " << unresolved << "\n";
-		f << "# bin_index  cap_dt[s]  cap_v2dt[km2/s]  cap_err_dt[s]  cap_err_v2dt[km2/s]  not_cap_dt[s]  not_cap_v2dt[km2/s]  not_cap_err_dt[s]  not_cap_err_v2dt[km2/s]\n";
-		const double n_cap = static_cast<double>(c[DMS_CNT_CAPTURED]);
-		const double n_nc = static_cast<double>(c[DMS_CNT_COMPLETED_OUTWARD]);
-		const double* h = hist.data();
-		for(int b = 0; b < DMS_NUM_BINS; b++)
-		{
-			const double cdt = h[DMS_HIST_CAPTURED_DT * DMS_NUM_BINS + b], cv = h[DMS_HIST_CAPTURED_V2DT * DMS_NUM_BINS + b];
-			const double ndt = h[DMS_HIST_NOT_CAPTURED_DT * DMS_NUM_BINS + b], nv = h[DMS_HIST_NOT_CAPTURED_V2DT * DMS_NUM_BINS + b];
-			f << b << "\t" << std::scientific << std::setprecision(10) << cdt << "\t" << cv << "\t"
-			  << Snapshot_Bin_Error(cdt, h[DMS_HIST_CAPTURED_DT_SQ * DMS_NUM_BINS + b], n_cap) << "\t"
-			  << Snapshot_Bin_Error(cv, h[DMS_HIST_CAPTURED_V2DT_SQ * DMS_NUM_BINS + b], n_cap) << "\t" << ndt << "\t" << nv << "\t"
-			  << Snapshot_Bin_Error(ndt, h[DMS_HIST_NOT_CAPTURED_DT_SQ * DMS_NUM_BINS + b], n_nc) << "\t"
-			  << Snapshot_Bin_Error(nv, h[DMS_HIST_NOT_CAPTURED_V2DT_SQ * DMS_NUM_BINS + b], n_nc) << "\n";
-		}
+		Write_Bincount_Rows(f, hist.data(), static_cast<double>(c[DMS_CNT_CAPTURED]), static_cast<double>(c[DMS_CNT_COMPLETED_OUTWARD]));
 		if(!f.good())
 			return DMS_ERR_IO;
 	}
 	{
 		// Write_Final_Evaporation_Time_File, src/Data_Generation.cpp:292-348 (one rank: rank 0)
-		std::sort(events.begin(), events.end(), [](const dms_evaporation_event& a, const dms_evaporation_event& b) {
-			if(a.lifetime_unbinding != b.lifetime_unbinding)
-				return a.lifetime_unbinding < b.lifetime_unbinding;
-			return a.trajectory_id < b.trajectory_id;
-		});
+		std::sort(events.begin(), events.end(), Event_Order);
 		const std::string path = join("evaporation_times.txt");
 		const std::string tmp = path + ".final.tmp." + std::to_string(getpid());
 		std::ofstream f(tmp, std::ios::out | std::ios::trunc);

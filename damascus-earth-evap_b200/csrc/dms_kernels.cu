@@ -470,15 +470,6 @@ void Launch_Initial_States(const RunParams& p, cudaStream_t stream)
 
 void Launch_Trajectories(const RunParams& p, int blocks, int threads, cudaStream_t stream)
 {
-#ifdef DMS_L1_CARVEOUT
-	// the lane state lives in local memory: give the unified L1 / shared-memory array to L1
-	static bool carveout = false;
-	if(!carveout)
-	{
-		cudaFuncSetAttribute(trajectory_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, DMS_L1_CARVEOUT);
-		carveout = true;
-	}
-#endif
 	trajectory_kernel<<<blocks, threads, 0, stream>>>(p);
 }
 

@@ -376,15 +376,6 @@ __global__ void grid_to_float_kernel(const double* __restrict__ in, float* __res
 
 void Launch_Trajectories_Mixed(const RunParams& p, int blocks, int threads, cudaStream_t stream)
 {
-#ifdef DMS_L1_CARVEOUT
-	// the lane state lives in local memory: give the unified L1 / shared-memory array to L1
-	static bool carveout = false;
-	if(!carveout)
-	{
-		cudaFuncSetAttribute(trajectory_kernel_mixed, cudaFuncAttributePreferredSharedMemoryCarveout, DMS_L1_CARVEOUT);
-		carveout = true;
-	}
-#endif
 	trajectory_kernel_mixed<<<blocks, threads, 0, stream>>>(p);
 }
 

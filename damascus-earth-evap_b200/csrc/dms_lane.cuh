@@ -404,10 +404,12 @@ __device__ __noinline__ void finalize(const RunParams& R, const DevPoint* __rest
 					const unsigned long long k = atomicAdd(R.event_count + L.point, 1ULL);
 					if(k < R.event_capacity)
 					{
-						dms_evaporation_event ev;
-						ev.trajectory_id = L.D.traj + 1;
+						// the lifetime is made visible before the id: a reader of a run in flight
+						// takes a slot whose id is still 0 (ids start at 1) as not yet published
+						dms_evaporation_event& ev = R.events[static_cast<size_t>(L.point) * R.event_capacity + k];
 						ev.lifetime_unbinding = lifetime;
-						R.events[static_cast<size_t>(L.point) * R.event_capacity + k] = ev;
+						__threadfence();
+						*reinterpret_cast<volatile uint64_t*>(&ev.trajectory_id) = L.D.traj + 1;
 					}
 					else
 						atomicAdd(c + DMS_CNT_EVENTS_DROPPED, 1ULL);

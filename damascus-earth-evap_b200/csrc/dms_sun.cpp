@@ -91,15 +91,24 @@ int main(int argc, char* argv[])
 	g.capture_mode = cfg.capture_mode ? 1 : 0;
 	g.max_scatterings = cfg.maximum_number_of_scatterings;
 	g.sigma_p_cm2 = cfg.sigma_nucleon_cm2;
+	// output path, src/main.cpp:89-92 (std::to_string of log10 values); snapshots go to its
+	// snapshot/ folder (src/Data_Generation.cpp:522-529)
+	const std::string out = cfg.output_dir + "results_" + std::to_string(std::log10(cfg.DM_mass_gev)) + "_" +
+	                        std::to_string(std::log10(cfg.sigma_nucleon_cm2)) + "/";
+	const std::string snapshot_dir = out + "snapshot/";
+	if(cfg.snapshot_enabled && !cfg.capture_mode)
+	{
+		g.snapshot_dir = snapshot_dir.c_str();
+		g.snapshot_interval_s = cfg.snapshot_interval;
+		g.snapshot_mass_gev = cfg.DM_mass_gev;
+		g.snapshot_sigma_cm2 = cfg.sigma_nucleon_cm2;
+	}
 	dms_generate_summary s;
 	if(dms_generate_data(ctx, pid, &g, &s) != DMS_OK)
 		return fail("dms_generate_data");
 	dms_print_summary(ctx, pid, &s, g.capture_mode);
 	if(!cfg.capture_mode)
 	{
-		// output path, src/main.cpp:89-92 (std::to_string of log10 values)
-		const std::string out = cfg.output_dir + "results_" + std::to_string(std::log10(cfg.DM_mass_gev)) + "_" +
-		                        std::to_string(std::log10(cfg.sigma_nucleon_cm2)) + "/";
 		if(dms_write_outputs(ctx, pid, &s, cfg.DM_mass_gev, cfg.sigma_nucleon_cm2, out.c_str()) != DMS_OK)
 			std::cerr << "Warning: failed to write the output files into " << out << std::endl;
 		// reflection spectrum, src/main.cpp:95-99

@@ -77,6 +77,15 @@ class PointResults(ctypes.Structure):
                 ("reflections_capacity", ctypes.c_uint64), ("reflections_count", ctypes.c_uint64)]
 
 
+class Progress(ctypes.Structure):
+    _fields_ = [("running", ctypes.c_int32), ("reserved", ctypes.c_int32), ("total", ctypes.c_uint64),
+                ("dispatched", ctypes.c_uint64), ("elapsed_s", ctypes.c_double)]
+
+
+# int (*dms_progress_fn)(dms_ctx*, void*)
+PROGRESS_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p)
+
+
 class ReflectionSpectrum(ctypes.Structure):
     _fields_ = [("trajectories", ctypes.c_uint64), ("reflections", ctypes.c_uint64), ("reflection_ratio", ctypes.c_double),
                 ("entering_rate_per_s", ctypes.c_double), ("reflection_rate_per_s", ctypes.c_double),
@@ -127,6 +136,9 @@ def library():
     lib.dms_measure_fp64_peak.argtypes = [vp, c.POINTER(c.c_double)]
     lib.dms_get_reflection_spectrum.argtypes = [vp, c.c_int, c.c_uint32, c.c_uint32, c.c_double, c.POINTER(ReflectionSpectrum)]
     lib.dms_reflection_spectrum_pdf.argtypes = [vp, c.c_int, c.c_uint32, c.c_uint32, vp, c.c_size_t, vp]
+    lib.dms_set_progress_callback.argtypes = [vp, PROGRESS_FN, vp, c.c_double]
+    lib.dms_peek_progress.argtypes = [vp, c.POINTER(Progress)]
+    lib.dms_peek_results.argtypes = [vp, c.c_int, c.POINTER(PointResults)]
     _lib = lib
     return lib
 
@@ -236,6 +248,40 @@ class Engine:
         return out
 
     def results(self, point, events_capacity=1 << 20, reflections_capacity=0):
+        """Accumulated results of a point (dms_get_results)."""
+        return self._results(self.lib.dms_get_results, point, events_capacity, reflections_capacity)
+
+    def peek_results(self, point, events_capacity=1 << 20):
+        """Results of the trajectories finished so far while a launch is in flight, from inside a
+        progress callback (dms_peek_results): `events` holds the published prefix."""
+        return self._results(self.lib.dms_peek_results, point, events_capacity, 0)
+
+    def peek_progress(self):
+        p = Progress()
+        self._check(self.lib.dms_peek_progress(self.h, ctypes.byref(p)))
+        return {"running": bool(p.running), "total": int(p.total), "dispatched": int(p.dispatched),
+                "elapsed_s": p.elapsed_s}
+
+    def set_progress_callback(self, fn, interval_s=1.0):
+        """Calls fn(engine) about every interval_s seconds while `run` / `run_records` wait for a
+        launch, on the calling thread; a true return (or an exception) cancels the run.  None
+        removes the hook."""
+        if fn is None:
+            self._check(self.lib.dms_set_progress_callback(self.h, PROGRESS_FN(), None, 0.0))
+            self._progress = None
+            return
+
+        def hook(ctx, user):
+            try:
+                return 1 if fn(self) else 0
+            except Exception as e:  # an exception cannot cross the C frames: cancel instead
+                self.progress_error = e
+                return 1
+        self.progress_error = None
+        self._progress = PROGRESS_FN(hook)  # kept alive while the library holds the pointer
+        self._check(self.lib.dms_set_progress_callback(self.h, self._progress, None, interval_s))
+
+    def _results(self, getter, point, events_capacity, reflections_capacity):
         res = PointResults()
         hist = np.zeros(NUM_HISTS * NUM_BINS)
         events = (EvaporationEvent * events_capacity)()
@@ -246,7 +292,7 @@ class Engine:
         res.events_capacity = events_capacity
         res.reflections = refl.ctypes.data_as(ctypes.POINTER(Reflection))
         res.reflections_capacity = reflections_capacity
-        self._check(self.lib.dms_get_results(self.h, point, ctypes.byref(res)))
+        self._check(getter(self.h, point, ctypes.byref(res)))
         counters = {name: int(res.counters[k]) for k, name in COUNTER_NAMES.items()}
         counters["reasons"] = [int(res.counters[REASON_BASE + k]) for k in range(11)]
         n = min(res.events_count, events_capacity)

@@ -16,6 +16,10 @@
  *   dms_get_results        Simulation_Data accumulators after Perform_MPI_Reductions
  *                                                                    src/Data_Generation.cpp:974-1210
  *   dms_rate               Solar_Model::Total_DM_Scattering_Rate     include/Solar_Model.hpp:334
+ *   dms_set_progress_callback, dms_peek_progress, dms_peek_results
+ *                          SnapshotRecorder + SnapshotHeartbeat (live progress of a run)
+ *                                                                    src/Snapshot_Shared_State.cpp:65-164,
+ *                                                                    src/Snapshot_Heartbeat.cpp:236-270
  *
  * Conventions: every call returns DMS_OK (0) or a negative DMS_ERR_* code, and the message of
  * the last failure is available from dms_last_error().  No C++ exception crosses the ABI.
@@ -288,6 +292,34 @@ typedef struct
 
 int dms_get_results(dms_ctx* ctx, int point_id, dms_point_results* results);
 int dms_reset_results(dms_ctx* ctx, int point_id);
+
+/* ---- Progress while a run is in flight ------------------------------------------------------
+ * Replaces the per-step SnapshotRecorder hooks and the heartbeat thread
+ * (src/Snapshot_Shared_State.cpp:65-78, src/Snapshot_Heartbeat.cpp:236-270): the kernel takes no
+ * per-step hook; instead the thread that called dms_run (or dms_run_records) polls the launch
+ * and calls fn about every interval_s seconds of wall time until the kernel ends.  fn may call
+ * dms_peek_progress and dms_peek_results, and nothing else of this API; a non-zero return
+ * cancels the run (dms_run then returns DMS_ERR_CANCELLED).  fn = NULL removes the hook. */
+typedef int (*dms_progress_fn)(dms_ctx* ctx, void* user);
+int dms_set_progress_callback(dms_ctx* ctx, dms_progress_fn fn, void* user, double interval_s);
+
+typedef struct
+{
+	int32_t running;        /* 1 while a launch is in flight */
+	int32_t reserved;
+	uint64_t total;         /* work items of the launch in flight (or of the last one) */
+	uint64_t dispatched;    /* work items taken by lanes so far, at most total */
+	double elapsed_s;       /* wall time since the launch began */
+} dms_progress;
+int dms_peek_progress(dms_ctx* ctx, dms_progress* progress);
+
+/* dms_get_results for a run in flight: counters and histograms of the trajectories finished so
+ * far, read on a second stream beside the running kernel, and the evaporation events published
+ * so far.  events_count is the number of leading published events copied (an event that another
+ * lane is still writing ends the prefix; it is published by a later call).  The view is for
+ * progress reports only: a trajectory finishing during the copy may be counted without its
+ * histogram rows, or the reverse.  Reflections are not part of it (reflections_count = 0). */
+int dms_peek_results(dms_ctx* ctx, int point_id, dms_point_results* results);
 
 /* Sizes a caller needs to know. */
 int dms_num_bins(void);

@@ -9,6 +9,9 @@
  *                       (bincount.txt, evaporation_times.txt)    src/Data_Generation.cpp:1212-1300
  *   dms_print_summary   Print_Summary / Print_Capture_Mode_Summary
  *                                                                src/Data_Generation.cpp:1366-1499
+ *   snapshot_* options  SnapshotHeartbeat + Snapshot_IO reports  src/Snapshot_Heartbeat.cpp:236-354,
+ *                       (snapshot/snapshot_{t}s.txt and          src/Snapshot_IO.cpp:508-650, 925-947
+ *                       snapshot_{t}s_evaporation_times.txt)
  */
 #ifndef DMS_DRIVER_H
 #define DMS_DRIVER_H
@@ -41,6 +44,15 @@ typedef struct
 	double time_limit_s;         /* per launch, 0 = none */
 	uint32_t threads_per_block;  /* 0 = default */
 	uint32_t blocks_per_sm;      /* 0 = default */
+	/* Wall-clock progress reports (snapshot_enabled / snapshot_interval of the configuration):
+	 * with snapshot_dir set and snapshot_interval_s a positive whole number of seconds, the
+	 * k-th report is written to snapshot_dir/snapshot_{k*interval}s.txt, with the evaporation
+	 * events first seen by it in snapshot_{k*interval}s_evaporation_times.txt.  Ignored in
+	 * capture mode (src/Data_Generation.cpp:490-491).  mass and sigma go into the headers. */
+	const char* snapshot_dir;    /* NULL = no snapshots */
+	double snapshot_interval_s;
+	double snapshot_mass_gev;
+	double snapshot_sigma_cm2;
 } dms_generate_opts;
 
 typedef struct

@@ -68,6 +68,8 @@ def test_usage_without_arguments():
     ({"DM_interaction": '"SD"'}, "is not provided by this engine (SI contact is)."),
     ({"DM_light": "false"}, "DM_light = false"),
     ({"maximum_number_of_scatterings": "1.5"}, "'maximum_number_of_scatterings' must be a non-negative integer."),
+    ({"snapshot_enabled": "true", "snapshot_interval": "0.5"}, "'snapshot_interval' must be a positive integer number of seconds."),
+    ({"snapshot_enabled": "true", "snapshot_interval": '"often"'}, "'snapshot_interval' must be a numeric value."),
 ])
 def test_configuration_errors(tmp_path, over, message):
     p = run(write_config(tmp_path / "bad.cfg", **over), tmp_path, timeout=60)
@@ -115,3 +117,58 @@ def test_capture_run_prints_capture_summary(tmp_path):
     for label in ("CAPTURE MODE summary", "Simulated trajectories:", "Total # of scatterings:", "Captured particle rate [1/s]:"):
         assert label in p.stdout, p.stdout
     assert not [d for d in os.listdir(tmp_path) if d.startswith("results_")]
+
+
+def read_header(path):
+    head, rows = {}, []
+    for line in open(path):
+        if line.startswith("#"):
+            if "=" in line:
+                k, v = line[1:].split("=", 1)
+                head[k.strip()] = v.strip()
+        elif line.strip():
+            rows.append(line.split())
+    return head, rows
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_snapshot_reports_during_a_parameter_point_run(tmp_path):
+    # a run of a few seconds (a million trajectories at the replay point) with a report a second
+    p = run(write_config(tmp_path / "snap.cfg", sample_size="1000000000", max_trajectories="1000000",
+                         maximum_number_of_scatterings="1000000", snapshot_enabled="true", snapshot_interval="1"), tmp_path)
+    assert p.returncode == 0, p.stderr
+    out = tmp_path / [d for d in os.listdir(tmp_path) if d.startswith("results_")][0]
+    final, _ = read_header(out / "bincount.txt")
+    seconds = float(final["simulation_time_seconds"])
+    names = sorted(os.listdir(out / "snapshot"))
+    reports = sorted((int(n[len("snapshot_"):-len("s.txt")]) for n in names if n.endswith("s.txt") and "_evap" not in n))
+    assert reports == list(range(1, int(seconds) + 1)), (reports, seconds)
+    assert len(reports) >= 2, seconds
+    assert not [n for n in names if ".tmp." in n]
+    final_events = {}
+    for l in open(out / "evaporation_times.txt"):
+        if l.strip() and not l.startswith("#"):
+            r = l.split()
+            final_events[int(r[1])] = r[2]
+    totals, assigned = [], {}
+    for t in reports:
+        head, rows = read_header(out / "snapshot" / ("snapshot_%ds.txt" % t))
+        if head["snapshot_status"] == "missed_writer_delay":
+            continue
+        assert head["snapshot_status"] == "merged" and head["snapshot_target_wall_time_s"] == str(t)
+        assert head["snapshot_interval_s"] == "1.000"
+        for key in ("capture_rate_raw", "capture_rate_valid_CI_95_upper", "valid_trajectories", "numerical_failures"):
+            assert key in head
+        assert len(rows) == 2000 and all(len(r) == 9 for r in rows)
+        totals.append(int(head["total_trajectories"]))
+        ev_head, ev_rows = read_header(out / "snapshot" / ("snapshot_%ds_evaporation_times.txt" % t))
+        assert ev_head["format_version"] == "3" and ev_head["DIAGNOSTIC_ONLY"] == "1"
+        lifetimes = [float(r[2]) for r in ev_rows]
+        assert lifetimes == sorted(lifetimes)
+        for r in ev_rows:
+            assert int(r[1]) not in assigned     # each event in one report only
+            assigned[int(r[1])] = r[2]
+    assert totals == sorted(totals) and totals
+    assert totals[-1] <= int(final["total_trajectories"])
+    assert all(final_events.get(i) == v for i, v in assigned.items())
