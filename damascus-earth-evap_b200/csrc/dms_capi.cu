@@ -329,6 +329,10 @@ void Fill_Dev_Point(const PointConstants& c, double* grid, DevPoint& d)
 	d.grid = grid;
 	d.grid_n = c.grid_n;
 	for(int k = 0; k < DMS_NUM_TARGETS; k++) d.sigma_t[k] = c.sigma_target[k];
+	d.interaction = static_cast<int>(c.interaction);
+	d.ff_num = c.ff_num;
+	d.ff_m2 = c.ff_m2;
+	for(int k = 0; k <= DMS_NUM_TARGETS; k++) d.q2c[k] = c.q2c[k];
 }
 }	// namespace
 

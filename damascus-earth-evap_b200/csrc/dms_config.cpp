@@ -2,6 +2,9 @@
 // reference's Configuration (src/Parameter_Scan.cpp:90-471) where its tests grep for them.
 #include "dms_config.h"
 
+#include "../../include/dms.h"
+#include "../../include/dms_constants.h"
+
 #include <cctype>
 #include <cmath>
 #include <fstream>
@@ -229,6 +232,25 @@ struct Keys
 		return true;
 	}
 };
+
+// DM distribution: the Standard Halo Model settings
+std::string Load_Halo(const Keys& k, RunConfig& cfg)
+{
+	std::string dist = "SHM";
+	k.Str("DM_distribution", dist);
+	if(dist != "SHM")
+		return "Error: DM_distribution " + dist + " is not provided by this engine (SHM is).";
+	k.Number("DM_local_density", cfg.rho_local);
+	k.Number("SHM_v0", cfg.v0);
+	k.Number("SHM_vEscape", cfg.vesc);
+	if(const ConfigValue* v = k.Get("SHM_vObserver"))
+	{
+		if(v->kind != ConfigValue::List || v->items.size() != 3)
+			return "Error: 'SHM_vObserver' must be a list of three velocities.";
+		for(int i = 0; i < 3; i++) cfg.vobs[i] = v->items[i].number;
+	}
+	return "";
+}
 }	// namespace
 
 std::string Load_Run_Config(const std::string& path, RunConfig& cfg)
@@ -328,10 +350,42 @@ std::string Load_Run_Config(const std::string& path, RunConfig& cfg)
 	if(cfg.DM_interaction != "SI" && cfg.DM_interaction != "SD" && cfg.DM_interaction != "Dark photon")
 		return "Error in DaMaSCUS_SUN::Configuration::Construct_DM_Particle(): 'DM_interaction' setting " + cfg.DM_interaction +
 		       " in configuration file not recognized.";
-	if(cfg.DM_interaction != "SI")
-		return "Error: DM_interaction " + cfg.DM_interaction + " is not provided by this engine (SI contact is).";
+	if(cfg.DM_interaction == "SD")
+		return "Error: DM_interaction SD is not provided by this engine (SI and Dark photon are).";
 	if(!cfg.DM_light)
 		return "Error: DM_light = false (nuclear form factors) is not provided by this engine.";
+	if(cfg.DM_interaction == "Dark photon")
+	{
+		// Construct_DM_Particle_Dark_Photon, src/Parameter_Scan.cpp:473-520, and the form factors
+		// the dark photon accepts (src/Dark_Photon.cpp:75-88); Electric-Dipole and Long-Range stop
+		// at the first rate evaluation with an IR divergence (:167-172)
+		if(!k.Str("DM_form_factor", cfg.DM_form_factor))
+			return "Error in DaMaSCUS_SUN::Configuration::Construct_DM_Particle_DP(): No 'DM_form_factor' setting in configuration file.";
+		if(cfg.DM_form_factor == "General")
+		{
+			if(!k.Number("DM_mediator_mass", cfg.mediator_mass_mev))
+				return "Error in Configuration::Construct_DM_Particle_DP(): No 'DM_mediator_mass' setting in configuration file.";
+			if(!std::isfinite(cfg.mediator_mass_mev) || cfg.mediator_mass_mev <= 0.0)
+				return "Error in Configuration::Construct_DM_Particle_DP(): 'DM_mediator_mass' must be finite and positive for the General form factor.";
+			cfg.interaction = DMS_INTERACTION_DARK_PHOTON_GENERAL;
+		}
+		else if(cfg.DM_form_factor == "Electric-Dipole" || cfg.DM_form_factor == "Long-Range")
+			return "Error in obscura::DM_Particle_Dark_Photon::Sigma_Nucleus(): Divergence in the IR.";
+		else if(cfg.DM_form_factor == "Contact")
+			cfg.interaction = DMS_INTERACTION_DARK_PHOTON_CONTACT;
+		else
+			return "Error in obscura::DM_Particle_Dark_Photon::Set_FormFactor_DM(): Form factor " + cfg.DM_form_factor + " not recognized.";
+		if(!k.Number("DM_cross_section_electron", cfg.sigma_electron_cm2))
+			return "Error in Configuration::Construct_DM_Particle_DP(): No 'DM_cross_section_electron' setting in configuration file.";
+		if(!std::isfinite(cfg.sigma_electron_cm2) || cfg.sigma_electron_cm2 < 0.0)
+			return "Error in Configuration::Construct_DM_Particle(): DM cross sections must be finite and non-negative.";
+		// the proton cross section follows from the electron one (src/Dark_Photon.cpp:130-133, 157-161)
+		const double mu_p = cfg.DM_mass_gev * DMS_MPROTON_GEV / (cfg.DM_mass_gev + DMS_MPROTON_GEV);
+		const double mu_e = cfg.DM_mass_gev * DMS_MELECTRON_GEV / (cfg.DM_mass_gev + DMS_MELECTRON_GEV);
+		cfg.sigma_nucleon_cm2 = cfg.sigma_electron_cm2 * (mu_p / mu_e) * (mu_p / mu_e);
+		return Load_Halo(k, cfg);
+	}
+	cfg.interaction = DMS_INTERACTION_SI;
 	k.Bool("DM_isospin_conserved", cfg.DM_isospin_conserved);
 	if(!cfg.DM_isospin_conserved)
 	{
@@ -349,22 +403,8 @@ std::string Load_Run_Config(const std::string& path, RunConfig& cfg)
 		return "Error in Configuration::Construct_DM_Particle(): DM cross sections must be finite and non-negative.";
 	k.Str("DM_form_factor", cfg.DM_form_factor);
 	if(cfg.DM_form_factor != "Contact")
-		return "Error: DM_form_factor " + cfg.DM_form_factor + " is not provided by this engine (Contact is).";
-	// DM distribution (SHM)
-	std::string dist = "SHM";
-	k.Str("DM_distribution", dist);
-	if(dist != "SHM")
-		return "Error: DM_distribution " + dist + " is not provided by this engine (SHM is).";
-	k.Number("DM_local_density", cfg.rho_local);
-	k.Number("SHM_v0", cfg.v0);
-	k.Number("SHM_vEscape", cfg.vesc);
-	if(const ConfigValue* v = k.Get("SHM_vObserver"))
-	{
-		if(v->kind != ConfigValue::List || v->items.size() != 3)
-			return "Error: 'SHM_vObserver' must be a list of three velocities.";
-		for(int i = 0; i < 3; i++) cfg.vobs[i] = v->items[i].number;
-	}
-	return "";
+		return "Error: DM_form_factor " + cfg.DM_form_factor + " is not provided by this engine for SI (Contact is).";
+	return Load_Halo(k, cfg);
 }
 
 }	// namespace dms

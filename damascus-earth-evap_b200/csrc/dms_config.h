@@ -48,7 +48,7 @@ struct RunConfig
 	bool snapshot_enabled = false;
 	double snapshot_interval = 60.0;  // seconds; the reference's default when snapshots are on
 	std::string output_dir = "./";
-	// DM particle (SI contact, low-mass mode)
+	// DM particle (low-mass mode: SI contact or dark photon)
 	double DM_mass_gev = 0.0;
 	double DM_spin = 0.5;
 	double DM_fraction = 1.0;
@@ -59,6 +59,8 @@ struct RunConfig
 	double sigma_nucleon_cm2 = 0.0;
 	double sigma_electron_cm2 = 0.0;
 	std::string DM_form_factor = "Contact";
+	unsigned int interaction = 0;       // DMS_INTERACTION_*
+	double mediator_mass_mev = 0.0;     // DM_mediator_mass (dark photon, General form factor)
 	// halo
 	double rho_local = 0.4;
 	double v0 = 220.0, vesc = 544.0;

@@ -51,8 +51,10 @@ struct DevPoint
 	const double* grid;    // grid_n x grid_n, radius-major
 	const float* grid_f;   // FP32 image of grid (mixed-precision kernel)
 	int grid_n;
-	int pad;
+	int interaction;       // DMS_INTERACTION_*
+	double ff_num, ff_m2;  // General form factor: (q_ref^2 + m^2)^2 / m^2, m^2 [GeV^2]
 	double sigma_t[DMS_NUM_TARGETS];
+	double q2c[DMS_NUM_TARGETS + 1];  // 4 mu_k^2 / c^2; [63] the electron
 };
 
 struct Vec3
@@ -171,6 +173,18 @@ __device__ __forceinline__ double thermal_relative_speed(double temperature, dou
 	return v * ((1.0 + 2.0 * x2) * erf(x) / (2.0 * x2) + exp(-x2) / (sqrt_pi * x));
 }
 
+// Sigma_Total_Nucleus / Sigma_Total_Electron of channel k (k = 63: the electron) at DM speed v:
+// the contact cross section, times (q_ref^2 + m^2)^2 / (m^2 (m^2 + q_max^2)) for the dark
+// photon's General form factor (src/Dark_Photon.cpp:167-229), q_max^2 = 4 mu_k^2 v^2 / c^2.
+__device__ __forceinline__ double channel_sigma(const DevPoint* __restrict__ P, int k, double v)
+{
+	const double sigma = (k == DMS_NUM_TARGETS) ? __ldg(&P->sigma_e) : __ldg(&P->sigma_t[k]);
+	if(__ldg(&P->interaction) != DMS_INTERACTION_DARK_PHOTON_GENERAL)
+		return sigma;
+	const double q2 = __ldg(&P->q2c[k]) * (v * v);
+	return sigma * (__ldg(&P->ff_num) / (__ldg(&P->ff_m2) + q2));
+}
+
 // Total_DM_Scattering_Rate_Computed and its channels, src/Solar_Model.cpp:263-342; the
 // per-target rates are written to rates[] when non-null (Sample_Target)
 static __device__ __noinline__ double rate_computed(const DevSolar& S, const DevPoint* __restrict__ P, double r, double v, double* rates, double* rate_e)
@@ -193,7 +207,7 @@ static __device__ __noinline__ double rate_computed(const DevSolar& S, const Dev
 	const double dr = r - __ldg(S.r + i);
 	const double T = __ldg(S.temp + i) + dr * __ldg(S.temp_s + i);
 	const double ne = __ldg(S.ne + i) + dr * __ldg(S.ne_s + i);
-	double total = ne * __ldg(&P->sigma_e) * thermal_relative_speed(T, DMS_MELECTRON_GEV, v);
+	double total = ne * channel_sigma(P, DMS_NUM_TARGETS, v) * thermal_relative_speed(T, DMS_MELECTRON_GEV, v);
 	if(rate_e)
 		*rate_e = total;
 	const double* nt = S.nt + static_cast<size_t>(i) * DMS_NUM_TARGETS;
@@ -202,7 +216,7 @@ static __device__ __noinline__ double rate_computed(const DevSolar& S, const Dev
 	{
 		const double n = __ldg(nt + k) + dr * __ldg(ns + k);
 		const double m = __ldg(S.target_mass + k);
-		const double rk = n * __ldg(&P->sigma_t[k]) * thermal_relative_speed(T, m, v);
+		const double rk = n * channel_sigma(P, k, v) * thermal_relative_speed(T, m, v);
 		if(rates)
 			rates[k] = rk;
 		total += rk;
@@ -1028,16 +1042,28 @@ __device__ __forceinline__ bool unit_vector_at_angle(double cos_theta, double ph
 // One channel of Total_DM_Scattering_Rate_Computed (src/Solar_Model.cpp:263-303) at knot
 // interval i, offset dr and temperature T: k < DMS_NUM_TARGETS the isotope k, k ==
 // DMS_NUM_TARGETS the electrons.  Same expressions, in the same order, as rate_computed.
+// The scattering angle of channel k (k < 0: the electron), one draw: isotropic for the contact
+// interactions, the General form factor's closed form otherwise (src/Dark_Photon.cpp:286-325).
+__device__ __forceinline__ double sample_cos_alpha(const DevPoint* __restrict__ P, Draws& D, int k, double v)
+{
+	if(__ldg(&P->interaction) != DMS_INTERACTION_DARK_PHOTON_GENERAL)
+		return D.uniform(-1.0, 1.0);
+	const double xi = D.uniform(0.0, 1.0);
+	const double m2 = __ldg(&P->ff_m2);
+	const double q2 = __ldg(&P->q2c[k < 0 ? DMS_NUM_TARGETS : k]) * (v * v);
+	return (m2 * (2.0 * xi - 1.0) + q2 * xi) / (m2 + q2 * xi);
+}
+
 __device__ __forceinline__ double channel_rate(const DevSolar& S, const DevPoint* __restrict__ P, int i, double dr, double T, double v, int k)
 {
 	if(k == DMS_NUM_TARGETS)
 	{
 		const double ne = __ldg(S.ne + i) + dr * __ldg(S.ne_s + i);
-		return ne * __ldg(&P->sigma_e) * thermal_relative_speed(T, DMS_MELECTRON_GEV, v);
+		return ne * channel_sigma(P, k, v) * thermal_relative_speed(T, DMS_MELECTRON_GEV, v);
 	}
 	const size_t o = static_cast<size_t>(i) * DMS_NUM_TARGETS + k;
 	const double n = __ldg(S.nt + o) + dr * __ldg(S.nt_s + o);
-	return n * __ldg(&P->sigma_t[k]) * thermal_relative_speed(T, __ldg(S.target_mass + k), v);
+	return n * channel_sigma(P, k, v) * thermal_relative_speed(T, __ldg(S.target_mass + k), v);
 }
 
 constexpr int TARGET_FAILED = -2;
@@ -1078,8 +1104,8 @@ __device__ __forceinline__ int pick_from_fractions(Draws& D, const double* q)
 }
 
 
-// The rest of Scatter once the target is known: Sample_Target_Velocity, the isotropic
-// scattering angle and New_DM_Velocity, src/Simulation_Trajectory.cpp:1160-1269.  Returns
+// The rest of Scatter once the target is known: Sample_Target_Velocity, the scattering angle
+// and New_DM_Velocity, src/Simulation_Trajectory.cpp:1160-1269.  Returns
 // false where the reference throws.
 static __device__ __noinline__ bool scatter_with_target(const DevSolar& S, const DevPoint* __restrict__ P, Draws& D, Event& e, int target)
 {
@@ -1147,7 +1173,7 @@ static __device__ __noinline__ bool scatter_with_target(const DevSolar& S, const
 	const Vec3 vel_t = scale3(vT, unit_t);
 	if(!isfinite(norm3(vel_t)))
 		return false;
-	const double cos_alpha = D.uniform(-1.0, 1.0);
+	const double cos_alpha = sample_cos_alpha(P, D, target, vdm);
 	const double md = __ldg(&P->m_dm);
 	if(!isfinite(cos_alpha) || cos_alpha < -1.0 - 1.0e-12 || cos_alpha > 1.0 + 1.0e-12 || !isfinite(md) || md <= 0.0 ||
 	   !isfinite(norm3(e.v)) || !isfinite(norm3(vel_t)))

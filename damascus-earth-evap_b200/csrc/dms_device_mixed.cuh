@@ -435,13 +435,13 @@ __device__ __forceinline__ double channel_rate_f(const DevSolar& S, const DevPoi
 	float m;
 	if(k == DMS_NUM_TARGETS)
 	{
-		n_sigma = (__ldg(S.ne + i) + dr * __ldg(S.ne_s + i)) * __ldg(&P->sigma_e);
+		n_sigma = (__ldg(S.ne + i) + dr * __ldg(S.ne_s + i)) * channel_sigma(P, k, v);
 		m = static_cast<float>(DMS_MELECTRON_GEV);
 	}
 	else
 	{
 		const size_t o = static_cast<size_t>(i) * DMS_NUM_TARGETS + k;
-		n_sigma = (__ldg(S.nt + o) + dr * __ldg(S.nt_s + o)) * __ldg(&P->sigma_t[k]);
+		n_sigma = (__ldg(S.nt + o) + dr * __ldg(S.nt_s + o)) * channel_sigma(P, k, v);
 		m = static_cast<float>(__ldg(S.target_mass + k));
 	}
 	return n_sigma * static_cast<double>(thermal_relative_speed_f(static_cast<float>(T), m, static_cast<float>(v)));
@@ -525,7 +525,7 @@ static __device__ __noinline__ bool scatter_with_target_f(const DevSolar& S, con
 	if(!unit_vector_at_angle_f(mu, phi_t, vd, unit_t))
 		return false;
 	const F3 vel_t = f3(vT * unit_t.x, vT * unit_t.y, vT * unit_t.z);
-	const float cos_alpha = static_cast<float>(D.uniform(-1.0, 1.0));
+	const float cos_alpha = static_cast<float>(sample_cos_alpha(P, D, target, static_cast<double>(vdm)));
 	const float md = static_cast<float>(__ldg(&P->m_dm));
 	if(!isfinite(normf(vel_t)) || !isfinite(md) || md <= 0.0f)
 		return false;

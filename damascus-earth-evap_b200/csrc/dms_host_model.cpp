@@ -256,20 +256,51 @@ std::string Make_Point_Constants(const SolarTables& t, const dms_point_params& p
 		return "interpolation grid too large";
 	if(!(p.halo_v0_kms > 0.0) || !(p.halo_vesc_kms > 0.0))
 		return "halo v0 and v_esc must be positive";
+	if(p.interaction > DMS_INTERACTION_DARK_PHOTON_GENERAL)
+		return "unknown DM interaction model";
+	if(p.interaction == DMS_INTERACTION_DARK_PHOTON_GENERAL && !(p.mediator_mass_mev > 0.0 && std::isfinite(p.mediator_mass_mev)))
+		return "'DM_mediator_mass' must be finite and positive for the General form factor";
 	c.m_dm = p.mass_gev;
-	const double sigma_p = p.sigma_p_cm2 * 1.0e-10;
+	c.interaction = p.interaction;
+	const bool dark_photon = p.interaction != DMS_INTERACTION_SI;
 	const double mu_p = c.m_dm * DMS_MPROTON_GEV / (c.m_dm + DMS_MPROTON_GEV);
+	const double mu_e = c.m_dm * DMS_MELECTRON_GEV / (c.m_dm + DMS_MELECTRON_GEV);
+	c.sigma_e = p.sigma_e_cm2 * 1.0e-10;
+	// the dark photon's kinetic mixing ties its proton cross section to the electron one:
+	// sigma_p = sigma_e (mu_p/mu_e)^2 (Set_Sigma_Electron, Sigma_Proton, src/Dark_Photon.cpp:130-133, 157-161)
+	const double ratio_pe = mu_p / mu_e;
+	const double sigma_p = dark_photon ? c.sigma_e * ratio_pe * ratio_pe : p.sigma_p_cm2 * 1.0e-10;
 	for(int k = 0; k < DMS_NUM_TARGETS; k++)
 	{
-		// SI contact cross section in low-mass mode: sigma_p (mu_N/mu_p)^2 [Z + (f_n/f_p)(A - Z)]^2
+		// contact cross section in low-mass mode: sigma_p (mu_N/mu_p)^2 [Z + (f_n/f_p)(A - Z)]^2 for
+		// SI, sigma_p (mu_N/mu_p)^2 Z^2 for the dark photon (src/Dark_Photon.cpp:167-184)
 		const dms_target_isotope& iso = DMS_TARGET_ISOTOPES[k];
 		const double mN = t.target_mass_gev[k];
 		const double mu_N = c.m_dm * mN / (c.m_dm + mN);
-		const double coupling = iso.Z + p.fn_over_fp * (iso.A - iso.Z);
+		const double coupling = dark_photon ? static_cast<double>(iso.Z) : iso.Z + p.fn_over_fp * (iso.A - iso.Z);
 		const double ratio = mu_N / mu_p;
 		c.sigma_target[k] = sigma_p * ratio * ratio * coupling * coupling;
+		const double mc = mu_N / DMS_C_KMS;
+		c.q2c[k] = 4.0 * mc * mc;
 	}
-	c.sigma_e = p.sigma_e_cm2 * 1.0e-10;
+	{
+		const double mc = mu_e / DMS_C_KMS;
+		c.q2c[DMS_NUM_TARGETS] = 4.0 * mc * mc;
+	}
+	if(p.interaction == DMS_INTERACTION_DARK_PHOTON_GENERAL)
+	{
+		// (q_ref^2 + m^2)^2 / m^2 with q_ref = alpha m_e (src/Dark_Photon.cpp:15-16, 194-198)
+		const double m = p.mediator_mass_mev * 1.0e-3;
+		const double q_ref = DMS_ALPHA_EM * DMS_MELECTRON_GEV;
+		const double a = q_ref * q_ref + m * m;
+		c.ff_m2 = m * m;
+		c.ff_num = a * a / m / m;
+	}
+	else
+	{
+		c.ff_m2 = 0.0;
+		c.ff_num = 0.0;
+	}
 	c.v0 = p.halo_v0_kms;
 	c.vesc_halo = p.halo_vesc_kms;
 	for(int i = 0; i < 3; i++) c.vel_obs[i] = p.halo_vobs_kms[i];

@@ -46,6 +46,9 @@ struct PointConstants
 	double m_dm;                     // GeV
 	double sigma_target[DMS_NUM_TARGETS]; // km^2
 	double sigma_e;                  // km^2
+	unsigned int interaction;        // DMS_INTERACTION_*
+	double ff_num, ff_m2;            // General form factor: (q_ref^2 + m^2)^2 / m^2, m^2 [GeV^2]
+	double q2c[DMS_NUM_TARGETS + 1]; // 4 mu_k^2 / c^2 [GeV^2 s^2 / km^2]; [63] the electron
 	double v0, vesc_halo, vobs;      // km/s
 	double vel_obs[3];
 	double n_esc;

@@ -76,6 +76,8 @@ int main(int argc, char* argv[])
 	p.halo_vesc_kms = cfg.vesc;
 	for(int i = 0; i < 3; i++) p.halo_vobs_kms[i] = cfg.vobs[i];
 	p.interpolation_points = cfg.interpolation_points;
+	p.interaction = cfg.interaction;
+	p.mediator_mass_mev = cfg.mediator_mass_mev;
 	int pid = -1;
 	std::cout << (cfg.capture_mode ? "Generate data in CAPTURE MODE..." : "Generate data...") << std::endl
 	          << "\tm_DM [MeV]:\t" << cfg.DM_mass_gev * 1000.0 << "\t\tsigma_p [cm2]:\t" << cfg.sigma_nucleon_cm2 << std::endl

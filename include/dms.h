@@ -124,10 +124,29 @@ int dms_load_solar_model(dms_ctx* ctx, const char* path);
 int dms_solar_table(dms_ctx* ctx, int which, double* out, size_t capacity);
 
 /* ---- parameter points -------------------------------------------------------------------- */
+
+/* DM interaction models (low-mass mode, DM_light = true):
+ *   SI                    DM_Particle_Standard "SI" with a contact interaction:
+ *                         sigma_N = sigma_p (mu_N/mu_p)^2 [Z + (f_n/f_p)(A - Z)]^2, isotropic angle
+ *   DARK_PHOTON_CONTACT   DM_Particle_Dark_Photon, DM_form_factor "Contact"
+ *                         (src/Dark_Photon.cpp:157-184, 190-210): the cross sections follow from the
+ *                         electron one, sigma_p = sigma_e (mu_p/mu_e)^2 and
+ *                         sigma_N = sigma_p (mu_N/mu_p)^2 Z^2; isotropic angle
+ *   DARK_PHOTON_GENERAL   "General", a dark photon of mass DM_mediator_mass: the contact cross
+ *                         sections times (q_ref^2 + m^2)^2 / (m^2 (m^2 + q_max^2)) with
+ *                         q_ref = alpha m_e and q_max = 2 mu v (v the DM speed), and the scattering
+ *                         angle cos = (m^2 (2 xi - 1) + q_max^2 xi) / (m^2 + q_max^2 xi)
+ *                         (src/Dark_Photon.cpp:192-229, 302-325)
+ * For the dark photon, sigma_p_cm2 and fn_over_fp are not used (the reference reads only
+ * DM_cross_section_electron, src/Parameter_Scan.cpp:508-519). */
+#define DMS_INTERACTION_SI                   0
+#define DMS_INTERACTION_DARK_PHOTON_CONTACT  1
+#define DMS_INTERACTION_DARK_PHOTON_GENERAL  2
+
 typedef struct
 {
 	double mass_gev;                   /* DM_mass */
-	double sigma_p_cm2;                /* DM_cross_section_nucleon (SI contact, low-mass mode) */
+	double sigma_p_cm2;                /* DM_cross_section_nucleon (SI) */
 	double sigma_e_cm2;                /* DM_cross_section_electron */
 	double fn_over_fp;                 /* 1.0 when DM_isospin_conserved */
 	double halo_v0_kms;                /* SHM_v0 */
@@ -135,7 +154,8 @@ typedef struct
 	double halo_vobs_kms[3];           /* SHM_vObserver */
 	uint32_t interpolation_points;     /* N of the N x N total-rate grid; N < 2: no grid, every
 	                                      lookup sums the 64 channels (Total_DM_Scattering_Rate_Computed) */
-	uint32_t reserved;
+	uint32_t interaction;              /* DMS_INTERACTION_* */
+	double mediator_mass_mev;          /* DM_mediator_mass of DARK_PHOTON_GENERAL [MeV], > 0 */
 } dms_point_params;
 
 /* Adds a parameter point and builds its N x N total-rate grid on the device (one kernel,

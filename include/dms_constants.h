@@ -28,6 +28,7 @@
 #define DMS_MPROTON_GEV      0.93827208816           /* proton mass [GeV] */
 #define DMS_MELECTRON_GEV    0.51099895000e-3        /* electron mass [GeV] */
 #define DMS_MNUCLEON_GEV     0.93149410242           /* atomic mass unit [GeV]; isotope mass = A*u */
+#define DMS_ALPHA_EM         (1.0 / 137.035999084)   /* fine-structure constant (CODATA 2018) */
 
 /* G*M_sun [km^3/s^2]; the engine stores G*M(r) directly (gravitational parameter). */
 #define DMS_GMSUN_KM3S2      (DMS_G_SI * DMS_MSUN_KG * 1.0e-9)

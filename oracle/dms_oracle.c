@@ -129,6 +129,9 @@ struct dms_oracle
 	double m_dm;                       /* GeV */
 	double sigma_target[DMS_NUM_TARGETS]; /* km^2 */
 	double sigma_e;                    /* km^2 */
+	unsigned int interaction;          /* DMS_INTERACTION_* */
+	double ff_num, ff_m2;              /* General form factor: (q_ref^2 + m^2)^2 / m^2 and m^2 [GeV^2] */
+	double q2c[DMS_NUM_TARGETS + 1];   /* 4 mu_k^2 / c^2 [GeV^2 s^2/km^2], [63] the electron */
 	double v0, vesc_halo, vobs;        /* km/s */
 	vec3 vel_obs;
 	double n_esc;
@@ -390,6 +393,18 @@ static double thermal_relative_speed(double temperature, double mass_target, dou
 	return v * ((1.0 + 2.0 * x2) * erf(x) / (2.0 * x2) + exp(-x2) / (SQRT_PI * x));
 }
 
+/* Sigma_Total_Nucleus / Sigma_Total_Electron at DM speed v [km/s] of channel k (k = 63: the
+ * electron): the contact cross section, times (q_ref^2 + m^2)^2 / (m^2 (m^2 + q_max^2)) for the
+ * dark photon's General form factor (src/Dark_Photon.cpp:190-229), q_max^2 = 4 mu_k^2 v^2 / c^2. */
+static double channel_sigma(const dms_oracle* o, int k, double v)
+{
+	const double sigma = (k == DMS_NUM_TARGETS) ? o->sigma_e : o->sigma_target[k];
+	if(o->interaction != DMS_INTERACTION_DARK_PHOTON_GENERAL)
+		return sigma;
+	const double q2 = o->q2c[k] * (v * v);
+	return sigma * (o->ff_num / (o->ff_m2 + q2));
+}
+
 /* DM_Scattering_Rate_Electron / _Nucleus, src/Solar_Model.cpp:263-303 */
 static double rate_electron(const dms_oracle* o, double r, double v)
 {
@@ -402,7 +417,7 @@ static double rate_electron(const dms_oracle* o, double r, double v)
 	if(r > DMS_RSUN_KM)
 		return 0.0;
 	const double vrel = thermal_relative_speed(solar_temperature(o, r), DMS_MELECTRON_GEV, v);
-	return solar_density(&o->n_e, r) * o->sigma_e * vrel;
+	return solar_density(&o->n_e, r) * channel_sigma(o, DMS_NUM_TARGETS, v) * vrel;
 }
 
 static double rate_nucleus(const dms_oracle* o, double r, double v, int t)
@@ -416,7 +431,7 @@ static double rate_nucleus(const dms_oracle* o, double r, double v, int t)
 	if(r > DMS_RSUN_KM)
 		return 0.0;
 	const double vrel = thermal_relative_speed(solar_temperature(o, r), o->target_mass_gev[t], v);
-	return solar_density(&o->targets[t], r) * o->sigma_target[t] * vrel;
+	return solar_density(&o->targets[t], r) * channel_sigma(o, t, v) * vrel;
 }
 
 /* Total_DM_Scattering_Rate_Computed, src/Solar_Model.cpp:324-342 */
@@ -1696,7 +1711,9 @@ static int scatter(dms_oracle* o, event_t* e)
 	const vec3 vel_t = v_scale(vT, unit_t);
 	if(!isfinite(v_norm(vel_t)))
 		return 0;
-	/* scattering angle (SI contact, isotropic): one draw, oracle/shim/obscura/DM_Particle.hpp */
+	/* scattering angle, one draw: isotropic for the contact interactions (SI,
+	 * oracle/shim/obscura/DM_Particle.hpp; dark photon "Contact", 2 xi - 1), or the General
+	 * form factor's closed form (Sample_Scattering_Angle_*, src/Dark_Photon.cpp:286-325) */
 	if(o->trace != NULL && o->trace_length < o->trace_capacity)
 	{
 		o->trace[3 * o->trace_length + 0] = r;
@@ -1705,7 +1722,15 @@ static int scatter(dms_oracle* o, event_t* e)
 	}
 	if(o->trace != NULL)
 		o->trace_length++;
-	const double cos_alpha = sample_uniform(o, -1.0, 1.0);
+	double cos_alpha;
+	if(o->interaction == DMS_INTERACTION_DARK_PHOTON_GENERAL)
+	{
+		const double xi = sample_uniform(o, 0.0, 1.0);
+		const double q2 = o->q2c[target == -1 ? DMS_NUM_TARGETS : target] * (vdm * vdm);
+		cos_alpha = (o->ff_m2 * (2.0 * xi - 1.0) + q2 * xi) / (o->ff_m2 + q2 * xi);
+	}
+	else
+		cos_alpha = sample_uniform(o, -1.0, 1.0);
 	/* New_DM_Velocity :1228-1247 */
 	if(!isfinite(cos_alpha) || cos_alpha < -1.0 - 1.0e-12 || cos_alpha > 1.0 + 1.0e-12 || !isfinite(o->m_dm) || o->m_dm <= 0.0 ||
 	   !isfinite(v_norm(e->velocity)) || !isfinite(v_norm(vel_t)))
@@ -1917,20 +1942,49 @@ int dms_oracle_set_point(dms_oracle* o, const dms_point_params* p)
 {
 	if(!o || !p || !(p->mass_gev > 0.0))
 		return DMS_ERR_INVALID_ARGUMENT;
+	if(p->interaction > DMS_INTERACTION_DARK_PHOTON_GENERAL ||
+	   (p->interaction == DMS_INTERACTION_DARK_PHOTON_GENERAL && !(p->mediator_mass_mev > 0.0 && isfinite(p->mediator_mass_mev))))
+		return DMS_ERR_INVALID_ARGUMENT;
 	o->m_dm = p->mass_gev;
-	const double sigma_p = p->sigma_p_cm2 * 1.0e-10;
+	o->interaction = p->interaction;
+	const int dark_photon = p->interaction != DMS_INTERACTION_SI;
 	const double mu_p = o->m_dm * DMS_MPROTON_GEV / (o->m_dm + DMS_MPROTON_GEV);
+	const double mu_e = o->m_dm * DMS_MELECTRON_GEV / (o->m_dm + DMS_MELECTRON_GEV);
+	o->sigma_e = p->sigma_e_cm2 * 1.0e-10;
+	/* the dark photon's proton cross section follows from the electron one through the kinetic
+	 * mixing (Set_Sigma_Electron then Sigma_Proton, src/Dark_Photon.cpp:130-133, 157-161) */
+	const double ratio_pe = mu_p / mu_e;
+	const double sigma_p = dark_photon ? o->sigma_e * ratio_pe * ratio_pe : p->sigma_p_cm2 * 1.0e-10;
 	for(int t = 0; t < DMS_NUM_TARGETS; t++)
 	{
-		/* DM_Particle_SI::Sigma_Total_Nucleus restated (oracle/shim/obscura/DM_Particle.hpp) */
+		/* DM_Particle_SI::Sigma_Total_Nucleus restated (oracle/shim/obscura/DM_Particle.hpp), or the
+		 * dark photon's low-mass Sigma_Total_Nucleus, sigma_p (mu_N/mu_p)^2 Z^2 (src/Dark_Photon.cpp:167-184) */
 		const dms_target_isotope* iso = &DMS_TARGET_ISOTOPES[t];
 		const double mN = o->target_mass_gev[t];
 		const double mu_N = o->m_dm * mN / (o->m_dm + mN);
-		const double coupling = iso->Z + p->fn_over_fp * (iso->A - iso->Z);
+		const double coupling = dark_photon ? (double)iso->Z : iso->Z + p->fn_over_fp * (iso->A - iso->Z);
 		const double ratio = mu_N / mu_p;
 		o->sigma_target[t] = sigma_p * ratio * ratio * coupling * coupling;
+		const double mc = mu_N / DMS_C_KMS;
+		o->q2c[t] = 4.0 * mc * mc;
 	}
-	o->sigma_e = p->sigma_e_cm2 * 1.0e-10;
+	{
+		const double mc = mu_e / DMS_C_KMS;
+		o->q2c[DMS_NUM_TARGETS] = 4.0 * mc * mc;
+	}
+	if(p->interaction == DMS_INTERACTION_DARK_PHOTON_GENERAL)
+	{
+		const double m = p->mediator_mass_mev * 1.0e-3;
+		const double q_ref = DMS_ALPHA_EM * DMS_MELECTRON_GEV;
+		const double a = q_ref * q_ref + m * m;
+		o->ff_m2 = m * m;
+		o->ff_num = a * a / m / m;
+	}
+	else
+	{
+		o->ff_m2 = 0.0;
+		o->ff_num = 0.0;
+	}
 	o->v0 = p->halo_v0_kms;
 	o->vesc_halo = p->halo_vesc_kms;
 	o->vel_obs = v3(p->halo_vobs_kms[0], p->halo_vobs_kms[1], p->halo_vobs_kms[2]);

@@ -17,6 +17,7 @@
 #include <memory>
 #include <string>
 
+#include "Dark_Photon.hpp"
 #include "Data_Generation.hpp"
 #include "Simulation_Trajectory.hpp"
 #include "Simulation_Utilities.hpp"
@@ -35,7 +36,7 @@ using namespace libphysica::natural_units;
 namespace
 {
 std::unique_ptr<Solar_Model> g_ssm;
-std::unique_ptr<obscura::DM_Particle_SI> g_dm;
+std::unique_ptr<obscura::DM_Particle> g_dm;
 std::unique_ptr<obscura::Standard_Halo_Model> g_halo;
 std::string g_error;
 
@@ -78,11 +79,27 @@ int dms_ref_set_point(const dms_point_params* p)
 		return -1;
 	try
 	{
-		g_dm.reset(new obscura::DM_Particle_SI(p->mass_gev * GeV));
-		g_dm->Set_Low_Mass_Mode(true);
-		g_dm->Set_Sigma_Proton(p->sigma_p_cm2 * cm * cm);
-		g_dm->Set_Sigma_Electron(p->sigma_e_cm2 * cm * cm);
-		g_dm->Fix_Coupling_Ratio(1.0, p->fn_over_fp);
+		if(p->interaction == DMS_INTERACTION_SI)
+		{
+			auto* si = new obscura::DM_Particle_SI(p->mass_gev * GeV);
+			g_dm.reset(si);
+			si->Set_Low_Mass_Mode(true);
+			si->Set_Sigma_Proton(p->sigma_p_cm2 * cm * cm);
+			si->Set_Sigma_Electron(p->sigma_e_cm2 * cm * cm);
+			si->Fix_Coupling_Ratio(1.0, p->fn_over_fp);
+		}
+		else
+		{
+			// the steps of Configuration::Construct_DM_Particle for "Dark photon"
+			// (src/Parameter_Scan.cpp:386-471, 473-520)
+			auto* dp = new DM_Particle_Dark_Photon();
+			g_dm.reset(dp);
+			const bool general = p->interaction == DMS_INTERACTION_DARK_PHOTON_GENERAL;
+			dp->Set_FormFactor_DM(general ? "General" : "Contact", general ? p->mediator_mass_mev * MeV : -1.0);
+			dp->Set_Interaction_Parameter(p->sigma_e_cm2 * cm * cm, "Electrons");
+			dp->Set_Mass(p->mass_gev * GeV);
+			dp->Set_Low_Mass_Mode(true);
+		}
 		libphysica::Vector vobs({p->halo_vobs_kms[0] * km / sec, p->halo_vobs_kms[1] * km / sec, p->halo_vobs_kms[2] * km / sec});
 		g_halo.reset(new obscura::Standard_Halo_Model(p->halo_v0_kms * km / sec, p->halo_vesc_kms * km / sec, vobs));
 		g_ssm->Interpolate_Total_DM_Scattering_Rate(*g_dm, p->interpolation_points, p->interpolation_points);

@@ -17,6 +17,7 @@ struct Isotope
 	Isotope() {}
 	Isotope(unsigned int z, unsigned int a, double abund = 1.0);
 	void Print_Summary(unsigned int MPI_rank = 0) const;
+	double Helm_Form_Factor(double) const { return 1.0; }  // low-mass mode: never used
 };
 struct Nucleus
 {

@@ -301,6 +301,11 @@ double DM_Particle_SI::Sigma_Total_Nucleus(const Isotope& target, double, double
 
 double DM_Particle_SI::Sigma_Total_Electron(double, double) { return sigma_electron; }
 
+double DM_Particle::High_Mass_Not_Shimmed()
+{
+	throw std::logic_error("the oracle shim provides obscura's low-mass mode only");
+}
+
 double DM_Particle_SI::Sample_Scattering_Angle_Nucleus(std::mt19937& PRNG, const Isotope&, double vDM, double r)
 {
 	Record_Scatter(r, vDM);

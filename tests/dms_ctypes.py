@@ -39,14 +39,21 @@ class PointParams(ctypes.Structure):
     _fields_ = [("mass_gev", ctypes.c_double), ("sigma_p_cm2", ctypes.c_double), ("sigma_e_cm2", ctypes.c_double),
                 ("fn_over_fp", ctypes.c_double), ("halo_v0_kms", ctypes.c_double), ("halo_vesc_kms", ctypes.c_double),
                 ("halo_vobs_kms", ctypes.c_double * 3), ("interpolation_points", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("interaction", ctypes.c_uint32), ("mediator_mass_mev", ctypes.c_double)]
+
+
+INTERACTION_SI = 0
+INTERACTION_DARK_PHOTON_CONTACT = 1
+INTERACTION_DARK_PHOTON_GENERAL = 2
 
 
 def point_params(mass_gev, sigma_p_cm2, sigma_e_cm2=1e-80, interpolation_points=1000,
-                 v0=220.0, vesc=544.0, vobs=(11.1, 232.2, 7.3), fn_over_fp=1.0):
-    """SI contact point with the Standard Halo Model of tests/config_unittest.cfg:78-80."""
+                 v0=220.0, vesc=544.0, vobs=(11.1, 232.2, 7.3), fn_over_fp=1.0, interaction=INTERACTION_SI,
+                 mediator_mass_mev=0.0):
+    """A point with the Standard Halo Model of tests/config_unittest.cfg:78-80: SI contact by
+    default, or a dark photon (contact / General) driven by sigma_e_cm2."""
     return PointParams(mass_gev, sigma_p_cm2, sigma_e_cm2, fn_over_fp, v0, vesc, (ctypes.c_double * 3)(*vobs),
-                       interpolation_points, 0)
+                       interpolation_points, interaction, mediator_mass_mev)
 
 
 def records_to_dicts(records):

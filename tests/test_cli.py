@@ -1,6 +1,7 @@
 """The `dms_sun` command-line drop-in: configuration errors (CPU, the file is read before any
 CUDA call) and complete Parameter-point and Capture runs with their summary and output files
 (B200 required)."""
+import math
 import os
 import subprocess
 
@@ -65,10 +66,18 @@ def test_usage_without_arguments():
     ({"run_mode": '"Spectrum"'}, "Run mode Spectrum not recognized."),
     ({"interpolation_points": "-1"}, "'interpolation_points' must be non-negative."),
     ({"sample_size": None}, "No 'sample_size' setting in configuration file."),
-    ({"DM_interaction": '"SD"'}, "is not provided by this engine (SI contact is)."),
+    ({"DM_interaction": '"SD"'}, "is not provided by this engine (SI and Dark photon are)."),
     ({"DM_light": "false"}, "DM_light = false"),
     ({"maximum_number_of_scatterings": "1.5"}, "'maximum_number_of_scatterings' must be a non-negative integer."),
     ({"snapshot_enabled": "true", "snapshot_interval": "0.5"}, "'snapshot_interval' must be a positive integer number of seconds."),
+    ({"DM_interaction": '"Dark photon"', "DM_form_factor": None}, "No 'DM_form_factor' setting in configuration file."),
+    ({"DM_interaction": '"Dark photon"', "DM_form_factor": '"General"'}, "No 'DM_mediator_mass' setting in configuration file."),
+    ({"DM_interaction": '"Dark photon"', "DM_form_factor": '"General"', "DM_mediator_mass": "-1.0"},
+     "'DM_mediator_mass' must be finite and positive for the General form factor."),
+    ({"DM_interaction": '"Dark photon"', "DM_form_factor": '"Long-Range"'}, "Divergence in the IR."),
+    ({"DM_interaction": '"Dark photon"', "DM_form_factor": '"Anapole"'}, "Form factor Anapole not recognized."),
+    ({"DM_interaction": '"Dark photon"', "DM_cross_section_electron": None},
+     "No 'DM_cross_section_electron' setting in configuration file."),
     ({"snapshot_enabled": "true", "snapshot_interval": '"often"'}, "'snapshot_interval' must be a numeric value."),
 ])
 def test_configuration_errors(tmp_path, over, message):
@@ -106,6 +115,24 @@ def test_parameter_point_run_writes_reference_outputs(tmp_path):
     ev = [l.split() for l in open(out / "evaporation_times.txt") if l.strip() and not l.startswith("#")]
     assert "# format_version = 3" in open(out / "evaporation_times.txt").read()
     assert all(len(r) == 3 and float(r[2]) > 0.0 for r in ev)
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_dark_photon_parameter_point_run(tmp_path):
+    # the dark photon's proton cross section follows from the electron one, and names the output
+    # folder (src/Dark_Photon.cpp:130-133, 157-161; src/main.cpp:89-92)
+    p = run(write_config(tmp_path / "dp.cfg", DM_interaction='"Dark photon"', DM_form_factor='"General"',
+                         DM_mediator_mass="0.2", DM_mass="1.0", DM_cross_section_electron="2.0e-39",
+                         sample_size="16", max_trajectories="20000"), tmp_path)
+    assert p.returncode == 0, p.stderr
+    dirs = [d for d in os.listdir(tmp_path) if d.startswith("results_")]
+    assert len(dirs) == 1
+    mu_p = 1.0 * 0.93827208816 / (1.0 + 0.93827208816)
+    mu_e = 1.0 * 0.51099895e-3 / (1.0 + 0.51099895e-3)
+    assert dirs[0] == "results_%f_%f" % (0.0, math.log10(2.0e-39 * (mu_p / mu_e) ** 2))
+    head, rows = read_header(tmp_path / dirs[0] / "bincount.txt")
+    assert int(head["captured_particles"]) >= 16 and len(rows) == 2000
 
 
 @needs_cli

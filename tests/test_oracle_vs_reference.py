@@ -80,3 +80,47 @@ def test_first_scattering_agrees(oracle_golden_point, golden, mode):
         assert tr[0][2] == ref_tr[2]  # same draw index at the scattering
         errs.append(max(abs(tr[0][0] - ref_tr[0]) / ref_tr[0], abs(tr[0][1] - ref_tr[1]) / ref_tr[1]))
     assert errs and max(errs) < 1e-7 and float(np.median(errs)) < 1e-10
+
+
+DP_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_dark_photon.json")
+
+
+@pytest.fixture(scope="module")
+def dp_golden():
+    with open(DP_GOLDEN) as f:
+        return json.load(f)
+
+
+def _dp_point(p):
+    return point_params(p["mass_gev"], 0.0, sigma_e_cm2=p["sigma_e_cm2"], interpolation_points=200,
+                        interaction=p["interaction"], mediator_mass_mev=p["mediator_mass_mev"])
+
+
+@pytest.mark.parametrize("which", [0, 1, 2])
+def test_dark_photon_rates_match_reference(oracle, dp_golden, which):
+    """Channel and total rates of the dark photon (src/Dark_Photon.cpp:167-229 through
+    src/Solar_Model.cpp:263-342): the kinetic-mixing cross sections and the General form factor."""
+    p = dp_golden["points"][which]
+    oracle.set_point(_dp_point(p))
+    for i, r in enumerate(dp_golden["radii_km"]):
+        for j, v in enumerate(dp_golden["speeds_kms"]):
+            want = p["rates"][i][j]
+            got = [oracle.query(12, r, k, v) for k in dp_golden["channels"]] + [oracle.query(6, r, v)]
+            for a, b in zip(got, want):
+                assert a == pytest.approx(b, rel=1e-9, abs=0.0), (p["name"], r, v)
+    assert p["rates"][1][2][-1] > 0.0
+
+
+@pytest.mark.parametrize("which", [0, 1, 2])
+def test_dark_photon_outcomes_agree(oracle, dp_golden, which):
+    """Trajectory outcomes with the dark photon's scattering angles (isotropic for Contact, the
+    closed-form General sampler, src/Dark_Photon.cpp:286-325)."""
+    from dms_ctypes import records_to_dicts
+    p = dp_golden["points"][which]
+    oracle.set_point(_dp_point(p))
+    ref = p["records"]
+    mine = records_to_dicts(oracle.run_records(dp_golden["seed"], 0, 0, len(ref))["records"])
+    same = sum(_outcome(a) == _outcome(b) for a, b in zip(ref, mine))
+    assert same >= int(math.ceil(0.98 * len(ref))), (p["name"], same)
+    assert sum(1 for a in ref if a["flags"] & 2) == sum(1 for b in mine if b["flags"] & 2)
+    assert sum(a["nscat"] for a in ref) > len(ref)
