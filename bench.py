@@ -309,14 +309,20 @@ def run_engine_arm(args):
                 if "cancelled" not in str(e):
                     raise
             c = engine.results(solo, events_capacity=1)["counters"]
+            # counted algorithmic FP64 operations of the work done (the FLOP model below)
+            ops = (FLOP_PER_ATTEMPT * (c["rk_attempts"] + c["unfinished_rk_attempts"]) +
+                   FLOP_PER_STEP * (c["rk_steps"] + c["unfinished_rk_steps"]) +
+                   FLOP_PER_SCATTER * (c["total_scatterings"] + c["unfinished_scatterings"]) +
+                   FLOP_PER_TRAJ * c["trajectories"])
             return (engine.last_kernel_ms(), c["total_scatterings"] + c["unfinished_scatterings"],
-                    c["rk_steps"] + c["unfinished_rk_steps"])
+                    c["rk_steps"] + c["unfinished_rk_steps"], ops)
         for name, prec in (("fp64", fp64), ("mixed", mixed)):
-            t1, s1, n1 = window(prec, 0.5 * args.steady_seconds)
-            t2, s2, n2 = window(prec, 1.5 * args.steady_seconds)
+            t1, s1, n1, f1 = window(prec, 0.5 * args.steady_seconds)
+            t2, s2, n2, f2 = window(prec, 1.5 * args.steady_seconds)
             dt = (t2 - t1) * 1e-3
             steady[name] = {"scatterings_per_s": (s2 - s1) / dt, "steps_per_s": (n2 - n1) / dt,
-                            "windows_ms": [t1, t2]}
+                            "counted_tflops": (f2 - f1) / dt / 1e12, "windows_ms": [t1, t2]}
+        steady["fp64"]["fp64_pipe_frac"] = steady["fp64"]["counted_tflops"] / peak if peak > 0 else None
         steady["mixed_over_fp64"] = steady["mixed"]["scatterings_per_s"] / steady["fp64"]["scatterings_per_s"]
 
     c = tot["counters"]
