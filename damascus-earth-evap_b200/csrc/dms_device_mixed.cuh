@@ -100,21 +100,21 @@ __constant__ double RKF_E[6] = {16.0 / 135.0 - 25.0 / 216.0, 0.0, 6656.0 / 12825
                                 -9.0 / 50.0 + 1.0 / 5.0, 2.0 / 55.0};
 
 // One pass of the Runge_Kutta_45_Step retry loop (src/Simulation_Trajectory.cpp:1492-1600):
-// FP32 stages, FP64 error norm and state update.
+// FP32 stages, FP64 error norm and state update.  Unrolled: the six stages written out (a
+// lane that runs alone takes 8 % less time per step); otherwise one loop over the stages
+// (a shorter instruction stream while every lane is busy).  Both evaluate the same
+// operations in the same order.
+template <bool Unrolled>
 __device__ __forceinline__ int rk45_attempt_f(const DevSolar& S, const DevSolarF& F, PropF& p, int inner)
 {
 	const float dt = static_cast<float>(p.time_step);
 	const float r = static_cast<float>(p.radius), v = static_cast<float>(p.v_radial);
-	// stages as one loop with accumulators for the later stages (see rk45_attempt); the
-	// 4th-order increments in FP32, the (b5 - b4) error sums in FP64.  Unrolled: the FP32
-	// stages are short enough that the written-out form fits the instruction cache, and a lane
-	// that runs alone (the tail of a launch) takes 8 % less time per step.
+	// stages with accumulators for the later stages (see rk45_attempt); the 4th-order
+	// increments in FP32, the (b5 - b4) error sums in FP64
 	float R1 = r, R2 = r, R3 = r, R4 = r, R5 = r, V1 = v, V2 = v, V3 = v, V4 = v, V5 = v;
 	float dr4 = 0.0f, dv4 = 0.0f, dp4 = 0.0f;
 	double er = 0.0, ev = 0.0, ep = 0.0;
-#pragma unroll
-	for(int j = 0; j < 6; j++)
-	{
+	auto stage = [&](int j) {
 		const float ri = j == 0 ? r : j == 1 ? R1 : j == 2 ? R2 : j == 3 ? R3 : j == 4 ? R4 : R5;
 		const float vi = j == 0 ? v : j == 1 ? V1 : j == 2 ? V2 : j == 3 ? V3 : j == 4 ? V4 : V5;
 		float a, b;
@@ -133,6 +133,16 @@ __device__ __forceinline__ int rk45_attempt_f(const DevSolar& S, const DevSolarF
 		er += c * static_cast<double>(kr);
 		ev += c * static_cast<double>(kv);
 		ep += c * static_cast<double>(kp);
+	};
+	if constexpr(Unrolled)
+	{
+#pragma unroll
+		for(int j = 0; j < 6; j++) stage(j);
+	}
+	else
+	{
+#pragma unroll 1
+		for(int j = 0; j < 6; j++) stage(j);
 	}
 	const double e0 = fabs(er), e1 = fabs(ev), e2 = fabs(ep);
 	const bool finite_state = isfinite(dr4) && isfinite(dv4) && isfinite(dp4);

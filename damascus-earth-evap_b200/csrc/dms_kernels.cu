@@ -60,7 +60,8 @@ __device__ __forceinline__ double commit_event(const DevSolar& S, double m_dm, i
 // RK45 retry loop: when no step is in progress the pre-step bounds are applied and a step is
 // opened; every pass makes one RK45 attempt; only a finished step runs the optical-depth,
 // boundary and commit logic.  Returns the next phase of the lane.
-__device__ __forceinline__ int free_step(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L, double2* hist)
+__device__ __forceinline__ int free_step(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L, double2* hist,
+                                         int drained)
 {
 	const DevSolar& S = R.S;
 	const int capture_mode = R.capture_mode;
@@ -119,7 +120,9 @@ __device__ __forceinline__ int free_step(const RunParams& R, const DevPoint* __r
 		L.rk_inner = 0;
 	}
 	L.rk_inner++;
-#if DMS_RK_UNROLLED
+#if DMS_RK_UNROLLED == 2
+	const int rk = drained ? rk45_attempt_unrolled(S, L.pr, L.rk_inner) : rk45_attempt(S, L.pr, L.rk_inner);
+#elif DMS_RK_UNROLLED == 1
 	const int rk = rk45_attempt_unrolled(S, L.pr, L.rk_inner);
 #else
 	const int rk = rk45_attempt(S, L.pr, L.rk_inner);
@@ -374,9 +377,10 @@ __global__ void __launch_bounds__(128) initial_state_kernel(const RunParams R)
 
 struct StrictStep
 {
-	__device__ __forceinline__ int operator()(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L, double2* hist) const
+	__device__ __forceinline__ int operator()(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L, double2* hist,
+	                                          int drained) const
 	{
-		return free_step(R, P, m_dm, L, hist);
+		return free_step(R, P, m_dm, L, hist, drained);
 	}
 	__device__ __forceinline__ double channel(const DevSolar& S, const DevPoint* __restrict__ P, int i, double dr, double T, double v, int k) const
 	{

@@ -59,7 +59,8 @@ __device__ __forceinline__ double commit_event_mixed(const DevSolar& S, const De
 // RK45 retry loop: when no step is in progress the pre-step bounds are applied and a step is
 // opened; every pass makes one RK45 attempt; only a finished step runs the optical-depth,
 // boundary and commit logic.  Returns the next phase of the lane.
-__device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, MixedLane& L, double2* hist)
+__device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, MixedLane& L, double2* hist,
+                                               int drained)
 {
 	const DevSolar& S = R.S;
 	const DevSolarF F{R.sf_r, R.sf_gm, R.sf_gm_s, R.sf_vesc2, R.sf_vesc2_s};
@@ -124,7 +125,12 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 		L.rk_inner = 0;
 	}
 	L.rk_inner++;
-	const int rk = rk45_attempt_f(S, F, L.pr, L.rk_inner);
+#if DMS_RK_UNROLLED_MIXED == 2
+	const int rk = drained ? rk45_attempt_f<true>(S, F, L.pr, L.rk_inner) : rk45_attempt_f<false>(S, F, L.pr, L.rk_inner);
+#else
+	(void)drained;
+	const int rk = rk45_attempt_f<DMS_RK_UNROLLED_MIXED == 1>(S, F, L.pr, L.rk_inner);
+#endif
 	if(rk == RK_RETRY)
 		return PH_STEP;
 	L.in_rk = 0;
@@ -347,9 +353,10 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 
 struct MixedStep
 {
-	__device__ __forceinline__ int operator()(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, MixedLane& L, double2* hist) const
+	__device__ __forceinline__ int operator()(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, MixedLane& L, double2* hist,
+	                                          int drained) const
 	{
-		return free_step_mixed(R, P, m_dm, L, hist);
+		return free_step_mixed(R, P, m_dm, L, hist, drained);
 	}
 	__device__ __forceinline__ double channel(const DevSolar& S, const DevPoint* __restrict__ P, int i, double dr, double T, double v, int k) const
 	{

@@ -662,6 +662,12 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	double2* hist = R.lane_hist + static_cast<size_t>(lane_id) * DMS_NUM_BINS;
 	__shared__ double coop_rates[4][DMS_NUM_TARGETS + 1];  // blocks of at most 128 threads
 	double* rates = coop_rates[threadIdx.x >> 5];
+	// set once a lane of the block finds the work queue empty: the launch is in its tail, where
+	// the lanes left run alone and the free step takes its shorter-chain form
+	__shared__ int queue_drained;
+	if(threadIdx.x == 0)
+		queue_drained = 0;
+	__syncthreads();
 	Lane L;
 	FlushJob job;
 	job.b0 = 0;
@@ -699,13 +705,16 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 			base = __shfl_sync(mask, base, leader);
 			const uint64_t w = base + rank;
 			if(w >= R.total)
+			{
+				*reinterpret_cast<volatile int*>(&queue_drained) = 1;
 				break;
+			}
 			phase = start_trajectory(R, L, w, P, m_dm);
 		}
 		if(phase == PH_SEGMENT)
 			phase = segment_start(R, P, m_dm, L);
 		if(phase == PH_STEP)
-			phase = step(R, P, m_dm, L, hist);
+			phase = step(R, P, m_dm, L, hist, *reinterpret_cast<volatile int*>(&queue_drained));
 		// Scatterings wait until several lanes of the warp have one (or one has waited
 		// DMS_SCATTER_MAX_WAIT iterations, or no lane is stepping), so that the scattering code
 		// runs for many lanes at once.  A lane's draws do not depend on when it scatters.
