@@ -5,6 +5,8 @@ import math
 import os
 import subprocess
 
+import numpy as np
+
 import pytest
 
 from dms_ctypes import PACKAGE_DIR
@@ -199,3 +201,40 @@ def test_snapshot_reports_during_a_parameter_point_run(tmp_path):
     assert totals == sorted(totals) and totals
     assert totals[-1] <= int(final["total_trajectories"])
     assert all(final_events.get(i) == v for i, v in assigned.items())
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_full_size_parameter_point_matches_one_launch(tmp_path):
+    """The Parameter-point configuration at its full size (run until 8192 captures, 1000 x 1000
+    grid, scatter cap 1e6, seed 7) through dms_sun, against the same trajectory ids in one
+    launch through the C ABI: the driver's rounds must not change any count (results are keyed
+    by trajectory id), and the file's invariants must hold."""
+    import sys
+    sys.path.insert(0, PACKAGE_DIR)
+    import dms_b200
+    p = run(write_config(tmp_path / "full.cfg", sample_size="8192", max_trajectories="0", interpolation_points="1000",
+                         maximum_number_of_scatterings="1000000", fixed_seed="7"), tmp_path)
+    assert p.returncode == 0, p.stderr
+    out = tmp_path / [d for d in os.listdir(tmp_path) if d.startswith("results_")][0]
+    head, rows = read_header(out / "bincount.txt")
+    total, captured = int(head["total_trajectories"]), int(head["captured_particles"])
+    valid, unresolved = int(head["valid_trajectories"]), int(head["unresolved_not_captured_trajectories"])
+    assert captured >= 8192 and valid + unresolved == total and valid >= captured
+    assert abs(float(head["capture_rate"]) - captured / total) < 1e-8
+    assert all(float(x) >= 0.0 for r in rows for x in r[1:])
+    ev = [l.split() for l in open(out / "evaporation_times.txt") if l.strip() and not l.startswith("#")]
+    lifetimes = [float(r[2]) for r in ev]
+    assert lifetimes == sorted(lifetimes) and 0 < len(ev) <= captured
+    with dms_b200.Engine(0) as e:
+        pid = e.add_point(dms_b200.point_params(0.3, 1e-36, interpolation_points=1000))
+        e.run([(pid, 0, total)], dms_b200.run_opts(seed=7, max_scatterings=10 ** 6, time_limit_s=600.0))
+        r = e.results(pid)
+    c = r["counters"]
+    assert c["trajectories"] == total and c["captured"] == captured
+    assert c["total_scatterings"] == int(head["total_scatterings"])
+    assert c["captured"] + c["completed_outward_escapes"] == valid
+    assert c["numerical_failures"] == int(head["numerical_failures"])
+    assert sorted(int(x[1]) for x in ev) == sorted(r["events"]["trajectory_id"].tolist())
+    cap_dt = np.array([float(x[1]) for x in rows])
+    assert np.allclose(cap_dt, r["histograms"][0], rtol=1e-9, atol=0)
