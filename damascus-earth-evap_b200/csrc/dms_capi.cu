@@ -85,6 +85,15 @@ int Fail(dms_ctx* ctx, int code, const std::string& msg)
 	return code;
 }
 
+// A progress callback runs while its launch is in flight; it may only peek.  Calls that would
+// reallocate or overwrite what the kernel uses are refused there.
+#define DMS_NOT_IN_FLIGHT(ctx)                                                                         \
+	do                                                                                                 \
+	{                                                                                                  \
+		if((ctx)->running)                                                                             \
+			return Fail((ctx), DMS_ERR_STATE, "not allowed while a launch is in flight (progress callback)"); \
+	} while(0)
+
 #define DMS_CUDA(ctx, call)                                                                                   \
 	do                                                                                                        \
 	{                                                                                                         \
@@ -284,10 +293,10 @@ int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 				cancelled_by_limit = true;
 			}
 		}
-		if(ctx->progress_fn && std::chrono::duration<double>(now - last_progress).count() >= ctx->progress_interval_s)
+		if(ctx->progress_fn && !cancelled_by_hook && std::chrono::duration<double>(now - last_progress).count() >= ctx->progress_interval_s)
 		{
 			last_progress = now;
-			if(ctx->progress_fn(ctx, ctx->progress_user) != 0 && !cancelled_by_hook)
+			if(ctx->progress_fn(ctx, ctx->progress_user) != 0)
 			{
 				*reinterpret_cast<volatile int*>(ctx->h_cancel) = 1;
 				cancelled_by_hook = true;
@@ -421,6 +430,7 @@ int dms_measure_fp64_peak(dms_ctx* ctx, double* tflops)
 {
 	if(!ctx || !tflops)
 		return DMS_ERR_INVALID_ARGUMENT;
+	DMS_NOT_IN_FLIGHT(ctx);
 	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
 	const double t = Measure_FP64_Peak(ctx->sm_count, ctx->stream);
 	if(!(t > 0.0))
@@ -441,6 +451,7 @@ int dms_load_solar_model(dms_ctx* ctx, const char* path)
 {
 	if(!ctx || !path)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	DMS_NOT_IN_FLIGHT(ctx);
 	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
 	SolarTables t;
 	const std::string err = Load_Solar_Tables(path, t);
@@ -553,6 +564,7 @@ int dms_add_point(dms_ctx* ctx, const dms_point_params* params, int* point_id)
 {
 	if(!ctx || !params)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	DMS_NOT_IN_FLIGHT(ctx);
 	if(!ctx->has_solar)
 		return Fail(ctx, DMS_ERR_NO_SOLAR_MODEL, "load a solar model before adding points");
 	if(static_cast<int>(ctx->points.size()) >= MAX_POINTS)
@@ -616,6 +628,7 @@ int dms_set_rate_grid(dms_ctx* ctx, int point_id, const double* grid, uint32_t n
 {
 	if(!ctx || !grid)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	DMS_NOT_IN_FLIGHT(ctx);
 	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
 		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
 	if(ctx->points[point_id].grid_n == 0)
@@ -645,6 +658,7 @@ int dms_rate(dms_ctx* ctx, int point_id, int interpolated, const double* r_km, c
 {
 	if(!ctx || (n > 0 && (!r_km || !v_kms || !rate_out)))
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null argument");
+	DMS_NOT_IN_FLIGHT(ctx);
 	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
 		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
 	if(n == 0)
@@ -684,6 +698,7 @@ int dms_run(dms_ctx* ctx, const dms_run_opts* opts, const dms_work_range* ranges
 {
 	if(!ctx)
 		return DMS_ERR_INVALID_ARGUMENT;
+	DMS_NOT_IN_FLIGHT(ctx);
 	int rc = Check_Run_Opts(ctx, opts);
 	if(rc != DMS_OK)
 		return rc;
@@ -742,6 +757,7 @@ int dms_run_records(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64
 {
 	if(!ctx)
 		return DMS_ERR_INVALID_ARGUMENT;
+	DMS_NOT_IN_FLIGHT(ctx);
 	int rc = Check_Run_Opts(ctx, opts);
 	if(rc != DMS_OK)
 		return rc;
@@ -841,6 +857,7 @@ int dms_reset_results(dms_ctx* ctx, int point_id)
 {
 	if(!ctx)
 		return DMS_ERR_INVALID_ARGUMENT;
+	DMS_NOT_IN_FLIGHT(ctx);
 	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
 		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
 	DMS_CUDA(ctx, cudaSetDevice(ctx->device));

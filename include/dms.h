@@ -318,8 +318,11 @@ int dms_reset_results(dms_ctx* ctx, int point_id);
  * (src/Snapshot_Shared_State.cpp:65-78, src/Snapshot_Heartbeat.cpp:236-270): the kernel takes no
  * per-step hook; instead the thread that called dms_run (or dms_run_records) polls the launch
  * and calls fn about every interval_s seconds of wall time until the kernel ends.  fn may call
- * dms_peek_progress and dms_peek_results, and nothing else of this API; a non-zero return
- * cancels the run (dms_run then returns DMS_ERR_CANCELLED).  fn = NULL removes the hook. */
+ * dms_peek_progress and dms_peek_results; the calls that launch work or change what the kernel
+ * reads (dms_run*, dms_add_point, dms_set_rate_grid, dms_reset_results, dms_rate,
+ * dms_load_solar_model, dms_measure_fp64_peak) return DMS_ERR_STATE there.  A non-zero return
+ * cancels the run (dms_run then returns DMS_ERR_CANCELLED) and ends the calls for that run.
+ * fn = NULL removes the hook. */
 typedef int (*dms_progress_fn)(dms_ctx* ctx, void* user);
 int dms_set_progress_callback(dms_ctx* ctx, dms_progress_fn fn, void* user, double interval_s);
 

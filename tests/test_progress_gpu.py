@@ -64,6 +64,32 @@ def test_progress_hook_reads_the_launch_in_flight(engine):
     assert e.peek_progress()["running"] is False
 
 
+def test_calls_that_change_the_launch_are_refused_in_the_hook(engine):
+    e, pid = engine
+    e.reset_results(pid)
+    refused = []
+
+    def hook(eng):
+        for call in (lambda: eng.add_point(dms_b200.point_params(0.3, 1e-36, interpolation_points=50)),
+                     lambda: eng.reset_results(pid),
+                     lambda: eng.run([(pid, 0, 4)], dms_b200.run_opts(seed=1))):
+            try:
+                call()
+            except dms_b200.EngineError as err:
+                refused.append("in flight" in str(err))
+        return True
+
+    e.set_progress_callback(hook, 0.05)
+    try:
+        with pytest.raises(dms_b200.EngineError, match="progress callback"):
+            e.run([(pid, 0, QUEUE)], dms_b200.run_opts(seed=3, max_scatterings=10 ** 6, time_limit_s=60.0))
+    finally:
+        e.set_progress_callback(None)
+    assert refused == [True, True, True]
+    n = e.lib.dms_num_points(e.h)
+    assert n == 1   # the refused add_point left no point behind
+
+
 def test_progress_hook_can_cancel(engine):
     e, pid = engine
     e.reset_results(pid)
