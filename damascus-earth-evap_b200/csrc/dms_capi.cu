@@ -206,6 +206,11 @@ int Check_Run_Opts(dms_ctx* ctx, const dms_run_opts* o)
 // limit through the mapped cancel flag.
 int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 {
+	if(!(o->max_trajectory_wall_time_s >= 0.0) || !std::isfinite(o->max_trajectory_wall_time_s))
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "'max_trajectory_wall_time_sec' must be finite and non-negative");
+	p.wall_limit_ns = static_cast<uint64_t>(o->max_trajectory_wall_time_s * 1.0e9);
+	if(o->max_trajectory_wall_time_s > 0.0 && p.wall_limit_ns == 0)
+		p.wall_limit_ns = 1;
 	const int threads = o->threads_per_block ? static_cast<int>(o->threads_per_block) : 128;
 	const bool mixed = o->precision == DMS_PRECISION_MIXED;
 	const int max_per_sm = mixed ? Trajectory_Mixed_Max_Blocks_Per_SM(threads) : Trajectory_Max_Blocks_Per_SM(threads);

@@ -80,6 +80,7 @@ struct RunParams
 	uint64_t max_free_steps;
 	double boundary;          // km
 	uint64_t iteration_budget;
+	uint64_t wall_limit_ns;  // per-trajectory wall-clock limit (max_trajectory_wall_time_sec); 0 = none
 	int ic_max_attempts;
 	// accumulators (accumulate mode)
 	unsigned long long* counters;   // n_points x DMS_NUM_COUNTERS

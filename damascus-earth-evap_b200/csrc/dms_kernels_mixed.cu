@@ -74,6 +74,11 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 			L.reason = DMS_REASON_MAX_FREE_STEPS;  // L.cur holds the last committed event
 			return PH_FINAL;
 		}
+		if(wall_time_exceeded(R, L))  // "before_step", src/Simulation_Trajectory.cpp:873-874
+		{
+			set_final(L, to_event64(prop_event_f(L.pr)), true, DMS_REASON_WALL_TIME_LIMIT);
+			return PH_FINAL;
+		}
 		if(!L.before_valid)
 		{
 			L.before = prop_event_f(L.pr);
@@ -155,6 +160,11 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 	if(v_after > DMS_V_MAX_C * DMS_C_KMS)
 	{
 		set_final(L, to_event64(after), true, DMS_REASON_SPEED_LIMIT);
+		return PH_FINAL;
+	}
+	if(wall_time_exceeded(R, L))  // "after_rk45_step", src/Simulation_Trajectory.cpp:953-954
+	{
+		set_final(L, to_event64(after), true, DMS_REASON_WALL_TIME_LIMIT);
 		return PH_FINAL;
 	}
 	bool scattering = false, reflection = false;

@@ -63,7 +63,24 @@ struct LaneT
 	// the bin being visited, held in registers until the trajectory leaves it
 	int cbin;
 	double2 cval;
+	uint64_t wall_start;  // %globaltimer at the start of the trajectory (wall-clock limit only)
 };
+// Nanoseconds of the device's global timer, one clock for every SM.
+__device__ __forceinline__ uint64_t global_timer_ns()
+{
+	uint64_t t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+// abort_if_wall_time_exceeded, src/Simulation_Trajectory.cpp:824-840: the trajectory's wall time
+// since it started on its lane against max_trajectory_wall_time_sec (0 = no limit)
+template <class Lane>
+__device__ __forceinline__ bool wall_time_exceeded(const RunParams& R, const Lane& L)
+{
+	return R.wall_limit_ns != 0 && global_timer_ns() - L.wall_start > R.wall_limit_ns;
+}
+
 template <class Lane>
 __device__ __forceinline__ void accumulate_bincount(Lane& L, double2* hist, double r, double v2, double dt)
 {
@@ -513,6 +530,7 @@ __device__ __forceinline__ int start_trajectory(const RunParams& R, Lane& L, uin
 	L.nscat = 0;
 	L.steps = 0;
 	L.attempts = 0;
+	L.wall_start = R.wall_limit_ns != 0 ? global_timer_ns() : 0;
 	L.is_captured = 0;
 	L.bound_state = 0;
 	L.t_capture = -1.0;

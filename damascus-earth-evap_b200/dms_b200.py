@@ -59,7 +59,8 @@ class RunOpts(ctypes.Structure):
                 ("max_free_steps", ctypes.c_uint64), ("boundary_radius_rsun", ctypes.c_double),
                 ("precision", ctypes.c_int32), ("threads_per_block", ctypes.c_uint32),
                 ("blocks_per_sm", ctypes.c_uint32), ("queue_chunk", ctypes.c_uint32),
-                ("iteration_budget", ctypes.c_uint64), ("time_limit_s", ctypes.c_double)]
+                ("iteration_budget", ctypes.c_uint64), ("time_limit_s", ctypes.c_double),
+                ("max_trajectory_wall_time_s", ctypes.c_double)]
 
 
 class WorkRange(ctypes.Structure):
@@ -154,7 +155,8 @@ PRECISION_MIXED = 1
 
 
 def run_opts(seed=1, capture_mode=False, max_scatterings=10 ** 14, max_free_steps=10 ** 12, boundary_rsun=2.0,
-             threads_per_block=0, blocks_per_sm=0, time_limit_s=0.0, iteration_budget=0, precision=PRECISION_FP64):
+             threads_per_block=0, blocks_per_sm=0, time_limit_s=0.0, iteration_budget=0, precision=PRECISION_FP64,
+             max_trajectory_wall_time_s=0.0):
     o = RunOpts()
     library().dms_default_run_opts(ctypes.byref(o))
     o.seed = seed
@@ -167,6 +169,7 @@ def run_opts(seed=1, capture_mode=False, max_scatterings=10 ** 14, max_free_step
     o.time_limit_s = time_limit_s
     o.iteration_budget = iteration_budget
     o.precision = precision
+    o.max_trajectory_wall_time_s = max_trajectory_wall_time_s
     return o
 
 

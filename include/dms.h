@@ -196,8 +196,11 @@ typedef struct
 	uint32_t queue_chunk;              /* trajectories claimed per queue fetch; 0 = default */
 	uint64_t iteration_budget;         /* per-lane loop-iteration bound; 0 = default */
 	double time_limit_s;               /* wall-clock bound of one launch, enforced through the
-	                                      cancel flag; 0 = none (the reference's
-	                                      max_trajectory_wall_time_sec is per trajectory) */
+	                                      cancel flag; 0 = none */
+	double max_trajectory_wall_time_s; /* max_trajectory_wall_time_sec: a trajectory whose wall time
+	                                      on its lane exceeds it ends with
+	                                      DMS_REASON_WALL_TIME_LIMIT (checked before and after each
+	                                      RK45 step, src/Simulation_Trajectory.cpp:824-840); 0 = none */
 } dms_run_opts;
 
 typedef struct

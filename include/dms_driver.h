@@ -42,6 +42,7 @@ typedef struct
 	double sigma_p_cm2;          /* selects the round granularity (the reference's sync interval) */
 	uint64_t round_capacity;     /* most trajectories per launch; 0 = 2^20 */
 	double time_limit_s;         /* per launch, 0 = none */
+	double max_trajectory_wall_time_s;  /* per trajectory (max_trajectory_wall_time_sec), 0 = none */
 	uint32_t threads_per_block;  /* 0 = default */
 	uint32_t blocks_per_sm;      /* 0 = default */
 	/* Wall-clock progress reports (snapshot_enabled / snapshot_interval of the configuration):

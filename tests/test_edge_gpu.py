@@ -18,7 +18,8 @@ from engine_fixtures import dms_b200, outcome, state
 
 pytestmark = pytest.mark.gpu
 
-REASON_MAX_SCATTERINGS = 5   # TrajectoryTerminationReason::MaxScatterings, include/dms.h
+REASON_WALL_TIME_LIMIT = 3   # TrajectoryTerminationReason::WallTimeLimit, include/dms.h
+REASON_MAX_SCATTERINGS = 5   # TrajectoryTerminationReason::MaxScatterings
 
 
 @pytest.fixture(scope="module")
@@ -102,3 +103,31 @@ def test_results_do_not_depend_on_the_range_split(engine):
         assert r["counters"] == out[0]["counters"]
         assert np.allclose(r["histograms"], out[0]["histograms"], rtol=1e-12, atol=0)
         assert sorted(r["events"]["trajectory_id"].tolist()) == sorted(out[0]["events"]["trajectory_id"].tolist())
+
+
+def test_trajectory_wall_time_limit(engine, oracle):
+    """max_trajectory_wall_time_sec (src/Simulation_Trajectory.cpp:824-840, 873-874, 953-954): a
+    trajectory whose wall time on its lane passes the limit ends with WallTimeLimit; every other
+    trajectory is untouched and replays the oracle (which has no limit) exactly."""
+    oracle.set_point(oracle_point_params(0.3, 1e-36, interpolation_points=300))
+    pid = engine.add_point(dms_b200.point_params(0.3, 1e-36, interpolation_points=300))
+    engine.set_rate_grid(pid, oracle.rate_grid())
+    n = 4096
+    opts = dms_b200.run_opts(seed=5, max_scatterings=10 ** 6, time_limit_s=120.0, max_trajectory_wall_time_s=0.002)
+    a = engine.run_records(pid, 0, n, opts)["records"]
+    b = oracle.run_records(5, pid, 0, n, max_scatterings=10 ** 6)["records"]
+    limited = [i for i in range(n) if a[i].termination_reason == REASON_WALL_TIME_LIMIT]
+    assert 0 < len(limited) < n
+    for i in range(n):
+        if i in limited:
+            assert a[i].number_of_draws <= b[i].number_of_draws
+            assert a[i].number_of_scatterings <= b[i].number_of_scatterings
+        else:
+            assert outcome(a[i]) == outcome(b[i]), i
+    engine.reset_results(pid)
+    engine.run([(pid, 0, n)], opts)
+    c = engine.results(pid, events_capacity=1)["counters"]
+    assert c["reasons"][REASON_WALL_TIME_LIMIT] > 0
+    assert c["computational_truncations"] >= c["reasons"][REASON_WALL_TIME_LIMIT]
+    with pytest.raises(dms_b200.EngineError, match="max_trajectory_wall_time_sec"):
+        engine.run([(pid, 0, 4)], dms_b200.run_opts(max_trajectory_wall_time_s=-1.0))
