@@ -193,8 +193,8 @@ int Check_Run_Opts(dms_ctx* ctx, const dms_run_opts* o)
 {
 	if(!o)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "null run options");
-	if(!(o->boundary_radius_rsun >= 1.0) || !std::isfinite(o->boundary_radius_rsun))
-		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "boundary radius must be at least one solar radius");
+	if(!(o->boundary_radius_rsun > 0.0) || !std::isfinite(o->boundary_radius_rsun))
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "boundary radius must be finite and positive");
 	if(o->precision != DMS_PRECISION_FP64 && o->precision != DMS_PRECISION_MIXED)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "unsupported precision");
 	if(o->threads_per_block != 0 && (o->threads_per_block % 32 != 0 || o->threads_per_block > 128))
@@ -260,6 +260,10 @@ int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 		p.sf_vesc2 = ctx->d_tables_f + 3 * static_cast<size_t>(ctx->dsolar.n);
 		p.sf_vesc2_s = ctx->d_tables_f + 4 * static_cast<size_t>(ctx->dsolar.n);
 	}
+#ifdef DMS_CHECKED
+	// bits left by a launch that does not report them (dms_run_records_noalloc) are dropped
+	(void)(mixed ? Take_Bounds_Status_Mixed() : Take_Bounds_Status());
+#endif
 	*ctx->h_cancel = 0;
 	DMS_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), ctx->stream));
 	DMS_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), ctx->stream));
@@ -322,6 +326,11 @@ int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 		return Fail(ctx, DMS_ERR_BUDGET, "run stopped: per-lane iteration budget exhausted");
 	if(status & STATUS_IC_REJECTION)
 		ctx->error = "warning: an initial-condition rejection loop hit its attempt bound";
+#ifdef DMS_CHECKED
+	const unsigned int bounds = mixed ? Take_Bounds_Status_Mixed() : Take_Bounds_Status();
+	if(bounds != 0)
+		return Fail(ctx, DMS_ERR_STATE, "checked build: an index left its bounds (bits " + std::to_string(bounds) + ")");
+#endif
 	return DMS_OK;
 }
 

@@ -18,6 +18,39 @@ namespace dms
 {
 
 // ---------------------------------------------------------------------------------------------
+// Checked build (-DDMS_CHECKED): every table, grid, histogram and work index is tested against
+// its bounds before use; a failure sets a bit of this translation unit's status word and the
+// index is clamped, so the kernel neither faults nor stops and the host reports the bits after
+// the launch.  The bits: 1 solar-table knot, 2 rate-grid cell, 4 histogram bin, 8 flushed
+// histogram row, 16 work range, 32 scattering target.  Without DMS_CHECKED the checks vanish.
+enum : unsigned int
+{
+	BOUNDS_KNOT = 1u,
+	BOUNDS_GRID = 2u,
+	BOUNDS_BIN = 4u,
+	BOUNDS_ROW = 8u,
+	BOUNDS_RANGE = 16u,
+	BOUNDS_TARGET = 32u,
+};
+#ifdef DMS_CHECKED
+static __device__ unsigned int dms_bounds_status;
+#define DMS_CHECK_INDEX(i, lo, hi, bit)                                  \
+	do                                                                   \
+	{                                                                    \
+		if(!((i) >= (lo) && (i) < (hi)))                                 \
+		{                                                                \
+			atomicOr(&dms_bounds_status, (bit));                         \
+			(i) = ((i) < (lo)) ? (lo) : (hi) - 1;                        \
+		}                                                                \
+	} while(0)
+#else
+#define DMS_CHECK_INDEX(i, lo, hi, bit) \
+	do                                  \
+	{                                   \
+	} while(0)
+#endif
+
+// ---------------------------------------------------------------------------------------------
 // Device images of the model
 struct DevSolar
 {
@@ -103,6 +136,7 @@ __device__ __forceinline__ int knot_index(const DevSolar& S, double x)
 	int b = static_cast<int>(x * S.bucket_scale);
 	b = b > S.nbuckets ? S.nbuckets : b;
 	int i = __ldg(S.bucket + b);
+	DMS_CHECK_INDEX(i, 0, last + 1, BOUNDS_KNOT);
 	while(i > 0 && __ldg(S.r + i) > x) i--;
 	while(i < last && __ldg(S.r + i + 1) <= x) i++;
 	return i;
@@ -245,6 +279,8 @@ __device__ __forceinline__ double rate_total(const DevSolar& S, const DevPoint* 
 	unsigned int vi = static_cast<unsigned int>(vc);
 	ri = ri > N - 2 ? N - 2 : ri;
 	vi = vi > N - 2 ? N - 2 : vi;
+	DMS_CHECK_INDEX(ri, 0u, N - 1, BOUNDS_GRID);
+	DMS_CHECK_INDEX(vi, 0u, N - 1, BOUNDS_GRID);
 	const double rf = rc - ri;
 	const double vf = vc - vi;
 	const double* g = reinterpret_cast<const double*>(__ldg(reinterpret_cast<const unsigned long long*>(&P->grid)));

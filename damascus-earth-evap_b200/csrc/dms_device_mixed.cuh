@@ -63,6 +63,7 @@ __device__ __forceinline__ int knot_index_f(const DevSolar& S, const DevSolarF& 
 	int b = static_cast<int>(x * static_cast<float>(S.bucket_scale));
 	b = b > S.nbuckets ? S.nbuckets : b;
 	int i = __ldg(S.bucket + b);
+	DMS_CHECK_INDEX(i, 0, last + 1, BOUNDS_KNOT);
 	while(i > 0 && __ldg(F.r + i) > x) i--;
 	while(i < last && __ldg(F.r + i + 1) <= x) i++;
 	return i;
@@ -298,6 +299,8 @@ __device__ __forceinline__ float rate_total_f(const DevSolar& S, const DevPoint*
 	unsigned int vi = static_cast<unsigned int>(vc);
 	ri = ri > N - 2 ? N - 2 : ri;
 	vi = vi > N - 2 ? N - 2 : vi;
+	DMS_CHECK_INDEX(ri, 0u, N - 1, BOUNDS_GRID);
+	DMS_CHECK_INDEX(vi, 0u, N - 1, BOUNDS_GRID);
 	const float rf = rc - ri, vf = vc - vi;
 	const size_t lower = static_cast<size_t>(ri) * N + vi;
 	const float g00 = __ldg(grid + lower), g01 = __ldg(grid + lower + 1);

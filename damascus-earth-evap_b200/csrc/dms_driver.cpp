@@ -476,6 +476,8 @@ int dms_generate_data(dms_ctx* ctx, int point_id, const dms_generate_opts* g, dm
 	opts.boundary_radius_rsun = g->boundary_radius_rsun;
 	opts.time_limit_s = g->time_limit_s;
 	opts.max_trajectory_wall_time_s = g->max_trajectory_wall_time_s;
+	if(g->max_free_steps != 0)
+		opts.max_free_steps = g->max_free_steps;
 	opts.threads_per_block = g->threads_per_block;
 	opts.blocks_per_sm = g->blocks_per_sm;
 	const uint64_t interval = g->capture_mode ? 32 : Sync_Interval(g->sigma_p_cm2);

@@ -366,7 +366,8 @@ __global__ void __launch_bounds__(128) initial_state_kernel(const RunParams R)
 	const uint64_t w = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
 	if(w >= R.total)
 		return;
-	const int k = find_range(R, w);
+	int k = find_range(R, w);
+	DMS_CHECK_INDEX(k, 0, R.n_ranges, BOUNDS_RANGE);
 	const int point = R.range_point[k];
 	Draws D;
 	D.seed = R.seed;
@@ -515,6 +516,20 @@ int Trajectory_Kernel_Registers()
 	if(cudaFuncGetAttributes(&a, trajectory_kernel) != cudaSuccess)
 		return -1;
 	return a.numRegs;
+}
+
+unsigned int Take_Bounds_Status()
+{
+#ifdef DMS_CHECKED
+	unsigned int bits = 0;
+	const unsigned int zero = 0;
+	if(cudaMemcpyFromSymbol(&bits, dms_bounds_status, sizeof bits) != cudaSuccess ||
+	   cudaMemcpyToSymbol(dms_bounds_status, &zero, sizeof zero) != cudaSuccess)
+		return ~0u;
+	return bits;
+#else
+	return 0;
+#endif
 }
 
 }	// namespace dms

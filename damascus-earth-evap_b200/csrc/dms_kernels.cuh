@@ -117,6 +117,11 @@ __device__ __forceinline__ int find_range(const RunParams& R, uint64_t w)
 	return lo;
 }
 
+// Checked build: reads and clears the bounds-status bits of the FP64 and the mixed kernels'
+// translation units (always 0 without DMS_CHECKED).
+unsigned int Take_Bounds_Status();
+unsigned int Take_Bounds_Status_Mixed();
+
 // Initial states of all p.total work indices into p.init (one thread per work index); the
 // trajectory kernels read them.  Launched on the same stream before every trajectory launch.
 void Launch_Initial_States(const RunParams& p, cudaStream_t stream);

@@ -409,4 +409,18 @@ int Trajectory_Mixed_Max_Blocks_Per_SM(int threads)
 	return n;
 }
 
+unsigned int Take_Bounds_Status_Mixed()
+{
+#ifdef DMS_CHECKED
+	unsigned int bits = 0;
+	const unsigned int zero = 0;
+	if(cudaMemcpyFromSymbol(&bits, dms_bounds_status, sizeof bits) != cudaSuccess ||
+	   cudaMemcpyToSymbol(dms_bounds_status, &zero, sizeof zero) != cudaSuccess)
+		return ~0u;
+	return bits;
+#else
+	return 0;
+#endif
+}
+
 }	// namespace dms

@@ -99,6 +99,7 @@ __device__ __forceinline__ void accumulate_bincount(Lane& L, double2* hist, doub
 	}
 	if(bin >= 0)
 	{
+		DMS_CHECK_INDEX(bin, 0, DMS_NUM_BINS, BOUNDS_BIN);
 		// The row is read only when a visited bin is entered again and written when it is
 		// left; the additions are the reference's, in its order.
 		if(bin != L.cbin)
@@ -483,8 +484,10 @@ __device__ __forceinline__ void cooperative_flush(double2* hist, FlushJob& job)
 		const int leader = __ffs(pending) - 1;
 		pending &= pending - 1u;
 		double2* row = reinterpret_cast<double2*>(__shfl_sync(grp, reinterpret_cast<unsigned long long>(hist), leader));
-		const int b0 = __shfl_sync(grp, job.b0, leader);
-		const int b1 = __shfl_sync(grp, job.b1, leader);
+		int b0 = __shfl_sync(grp, job.b0, leader);
+		int b1 = __shfl_sync(grp, job.b1, leader);
+		DMS_CHECK_INDEX(b0, 0, DMS_NUM_BINS, BOUNDS_ROW);
+		DMS_CHECK_INDEX(b1, 0, DMS_NUM_BINS, BOUNDS_ROW);
 		const int mode = __shfl_sync(grp, job.mode, leader);
 		double* d0 = reinterpret_cast<double*>(__shfl_sync(grp, reinterpret_cast<unsigned long long>(job.dst0), leader));
 		double* d1 = reinterpret_cast<double*>(__shfl_sync(grp, reinterpret_cast<unsigned long long>(job.dst1), leader));
@@ -518,7 +521,8 @@ __device__ __forceinline__ void cooperative_flush(double2* hist, FlushJob& job)
 template <class Lane>
 __device__ __forceinline__ int start_trajectory(const RunParams& R, Lane& L, uint64_t w, const DevPoint*& P, double& m_dm)
 {
-	const int k = find_range(R, w);
+	int k = find_range(R, w);
+	DMS_CHECK_INDEX(k, 0, R.n_ranges, BOUNDS_RANGE);
 	L.work = w;
 	L.point = R.range_point[k];
 	P = R.points + L.point;
@@ -637,6 +641,8 @@ __device__ __forceinline__ void cooperative_targets(const RunParams& R, Lane& L,
 template <class Lane, class Step>
 __device__ __forceinline__ int finish_scatter(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, Lane& L, int target, const Step& step)
 {
+	if(target != TARGET_FAILED)
+		DMS_CHECK_INDEX(target, -1, DMS_NUM_TARGETS, BOUNDS_TARGET);
 	if(target == TARGET_FAILED || !step.scatter(R.S, P, L.D, L.cur, target))
 	{
 		L.reason = DMS_REASON_NUMERICAL_FAILURE;

@@ -92,6 +92,28 @@ class Progress(ctypes.Structure):
 PROGRESS_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p)
 
 
+class GenerateOpts(ctypes.Structure):
+    _fields_ = [("sample_size", ctypes.c_uint32), ("max_trajectories", ctypes.c_uint32), ("seed", ctypes.c_uint32),
+                ("capture_mode", ctypes.c_int32), ("max_scatterings", ctypes.c_uint64),
+                ("boundary_radius_rsun", ctypes.c_double), ("sigma_p_cm2", ctypes.c_double),
+                ("round_capacity", ctypes.c_uint64), ("time_limit_s", ctypes.c_double),
+                ("max_trajectory_wall_time_s", ctypes.c_double), ("threads_per_block", ctypes.c_uint32),
+                ("blocks_per_sm", ctypes.c_uint32), ("snapshot_dir", ctypes.c_char_p),
+                ("snapshot_interval_s", ctypes.c_double), ("snapshot_mass_gev", ctypes.c_double),
+                ("snapshot_sigma_cm2", ctypes.c_double), ("max_free_steps", ctypes.c_uint64)]
+
+
+class GenerateSummary(ctypes.Structure):
+    _fields_ = [("counters", ctypes.c_uint64 * NUM_COUNTERS), ("rounds", ctypes.c_uint64),
+                ("final_round_trajectories", ctypes.c_uint64), ("capture_target_overshoot", ctypes.c_uint64),
+                ("sync_interval", ctypes.c_uint64), ("next_trajectory", ctypes.c_uint64),
+                ("early_stop_reason", ctypes.c_int32), ("reserved", ctypes.c_int32), ("computing_time_s", ctypes.c_double)]
+
+
+STOP_NAMES = {0: "none", 1: "max_trajectories_reached", 2: "capture_target_not_reached",
+              3: "initial_shift_failure_fraction_exceeded", 4: "invalid_trajectory_fraction_exceeded"}
+
+
 class ReflectionSpectrum(ctypes.Structure):
     _fields_ = [("trajectories", ctypes.c_uint64), ("reflections", ctypes.c_uint64), ("reflection_ratio", ctypes.c_double),
                 ("entering_rate_per_s", ctypes.c_double), ("reflection_rate_per_s", ctypes.c_double),
@@ -144,6 +166,10 @@ def library():
     lib.dms_get_reflection_spectrum.argtypes = [vp, c.c_int, c.c_uint32, c.c_uint32, c.c_double, c.POINTER(ReflectionSpectrum)]
     lib.dms_reflection_spectrum_pdf.argtypes = [vp, c.c_int, c.c_uint32, c.c_uint32, vp, c.c_size_t, vp]
     lib.dms_set_progress_callback.argtypes = [vp, PROGRESS_FN, vp, c.c_double]
+    lib.dms_default_generate_opts.argtypes = [c.POINTER(GenerateOpts)]
+    lib.dms_default_generate_opts.restype = None
+    lib.dms_generate_data.argtypes = [vp, c.c_int, c.POINTER(GenerateOpts), c.POINTER(GenerateSummary)]
+    lib.dms_write_outputs.argtypes = [vp, c.c_int, c.POINTER(GenerateSummary), c.c_double, c.c_double, c.c_char_p]
     lib.dms_peek_progress.argtypes = [vp, c.POINTER(Progress)]
     lib.dms_peek_results.argtypes = [vp, c.c_int, c.POINTER(PointResults)]
     _lib = lib
@@ -312,6 +338,30 @@ class Engine:
         if reflections_capacity:
             out["reflections"] = refl[:min(res.reflections_count, reflections_capacity)]
         return out
+
+    def generate(self, point, sample_size, max_trajectories=0, seed=0, capture_mode=False, max_scatterings=None,
+                 boundary_rsun=2.0, sigma_p_cm2=1e-36, max_free_steps=0, time_limit_s=0.0):
+        """Simulation_Data::Generate_Data through dms_generate_data: rounds until sample_size
+        captures, the trajectory budget or a run-level fuse; returns the summary."""
+        g = GenerateOpts()
+        self.lib.dms_default_generate_opts(ctypes.byref(g))
+        g.sample_size, g.max_trajectories, g.seed = sample_size, max_trajectories, seed
+        g.capture_mode = int(bool(capture_mode))
+        if max_scatterings is not None:
+            g.max_scatterings = max_scatterings
+        g.boundary_radius_rsun, g.sigma_p_cm2 = boundary_rsun, sigma_p_cm2
+        g.max_free_steps, g.time_limit_s = max_free_steps, time_limit_s
+        summary = GenerateSummary()
+        self._check(self.lib.dms_generate_data(self.h, point, ctypes.byref(g), ctypes.byref(summary)))
+        counters = {name: int(summary.counters[k]) for k, name in COUNTER_NAMES.items()}
+        counters["reasons"] = [int(summary.counters[REASON_BASE + k]) for k in range(11)]
+        return {"summary": summary, "counters": counters, "early_stop": STOP_NAMES[summary.early_stop_reason],
+                "rounds": int(summary.rounds), "computing_time_s": summary.computing_time_s}
+
+    def write_outputs(self, point, generated, mass_gev, sigma_cm2, directory):
+        """Write_Output_Files: bincount.txt and evaporation_times.txt into directory."""
+        self._check(self.lib.dms_write_outputs(self.h, point, ctypes.byref(generated["summary"]), mass_gev, sigma_cm2,
+                                               directory.encode()))
 
     def reflection_spectrum(self, point, rings=1, ring=0, dm_density_gev_cm3=0.4):
         s = ReflectionSpectrum()

@@ -38,7 +38,8 @@ typedef struct
 	uint32_t seed;               /* fixed_seed */
 	int32_t capture_mode;
 	uint64_t max_scatterings;    /* maximum_number_of_scatterings */
-	double boundary_radius_rsun; /* 2.0 */
+	double boundary_radius_rsun; /* initial_and_final_radius / R_sun of Configure (2.0); below 1 every
+	                                initial Kepler shift fails, as in the reference */
 	double sigma_p_cm2;          /* selects the round granularity (the reference's sync interval) */
 	uint64_t round_capacity;     /* most trajectories per launch; 0 = 2^20 */
 	double time_limit_s;         /* per launch, 0 = none */
@@ -54,6 +55,7 @@ typedef struct
 	double snapshot_interval_s;
 	double snapshot_mass_gev;
 	double snapshot_sigma_cm2;
+	uint64_t max_free_steps;     /* maximum_free_time_steps of Configure; 0 = the default (1e12) */
 } dms_generate_opts;
 
 typedef struct

@@ -114,7 +114,7 @@ def test_errors_leave_context_usable(engine, replay):
     with pytest.raises(dms_b200.EngineError):
         engine.run([(pid + 1000, 0, 10)], dms_b200.run_opts())
     with pytest.raises(dms_b200.EngineError):
-        engine.run([(pid, 0, 10)], dms_b200.run_opts(boundary_rsun=0.5))
+        engine.run([(pid, 0, 10)], dms_b200.run_opts(boundary_rsun=0.0))
     with pytest.raises(dms_b200.EngineError):
         engine.add_point(dms_b200.point_params(-1.0, 1e-36))
     # a wall-clock limit far below the run length cancels the launch; the context stays usable
