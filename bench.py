@@ -46,9 +46,10 @@ WORKLOAD = ("Parameter-point evaporation (config 1): SI contact m=0.3 GeV sigma_
 # conditions, Kepler shift, classification).
 FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ = 214.8, 622.3, 2455.0, 3374.0
 # DRAM bytes (read + write) of the FP64 trajectory kernel per trajectory of this point, from one
-# ncu capture of 2^19 trajectories (73 GB); almost all of it is the termination flush of the
-# per-lane histogram row.
-TRAFFIC_PER_TRAJECTORY = 73.0e9 / (1 << 19)
+# ncu capture of one 65 536-trajectory batch (ids 0-65 535: 2.52 GB read + 3.95 GB written, 435
+# bytes per accepted step): the lane state's local-memory traffic and the termination flush of
+# the per-lane histogram rows.
+TRAFFIC_PER_TRAJECTORY = (2524931584 + 3947619584) / 65536
 
 
 def log(*a):
@@ -364,8 +365,8 @@ def run_engine_arm(args):
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak > 0 else None,
                          "traffic": TRAFFIC_PER_TRAJECTORY * c["trajectories"],
-                         "traffic_source": "ncu dram__bytes of a 2^19-trajectory launch of this point, per trajectory x "
-                                           "trajectories of this launch",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 65536-trajectory "
+                                           "batch of this point, per trajectory x trajectories of this launch",
                          "peak_source": "measured in this run: DFMA-chain kernel on all SMs (2 FLOP per FMA)",
                          "flop_model": "%.1f/attempt + %.1f/step + %.0f/scattering + %.0f/trajectory (counted)" % (
                              FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ)},

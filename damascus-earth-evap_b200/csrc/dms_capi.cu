@@ -21,6 +21,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/dms.h"
 #include "../../include/dms_driver.h"
 #include "dms_host_model.h"
@@ -267,6 +269,13 @@ int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 	*ctx->h_cancel = 0;
 	DMS_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), ctx->stream));
 	DMS_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), ctx->stream));
+	// one NVTX range per launch, so that a profiler timeline shows each trajectory launch
+	const std::string range = std::string(mixed ? "dms mixed launch: " : "dms fp64 launch: ") + std::to_string(p.total) + " trajectories";
+	nvtxRangePushA(range.c_str());
+	struct Pop
+	{
+		~Pop() { nvtxRangePop(); }
+	} pop;
 	DMS_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
 	Launch_Initial_States(p, ctx->stream);
 	DMS_CUDA(ctx, cudaGetLastError());
