@@ -438,6 +438,46 @@ struct Hook_Guard
 	}
 };
 
+// print_progress_update, src/Data_Generation.cpp:661-694: one line when the captured fraction of
+// the requested sample passes a milestone, with a progress bar, the elapsed time and the capture
+// rate.  The bar is this library's own drawing (libphysica's is not part of the reference).
+class Progress_Printer
+{
+  public:
+	Progress_Printer(bool on, uint32_t requested, std::chrono::steady_clock::time_point t0) : on_(on), requested_(requested), t0_(t0) {}
+	void Update(uint64_t captured, bool force)
+	{
+		if(!on_)
+			return;
+		static const double milestones[] = {0.0, 0.01, 0.05, 0.10, 0.20, 0.40, 0.60, 0.80, 1.0};
+		const double progress = std::min(1.0, static_cast<double>(captured) / std::max<double>(1.0, requested_));
+		bool print = force;
+		while(next_ < sizeof milestones / sizeof milestones[0] && progress + 1.0e-12 >= milestones[next_])
+		{
+			print = true;
+			next_++;
+		}
+		if(!print || (force && printed_ && captured == last_))
+			return;
+		const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+		const int width = 44, filled = static_cast<int>(progress * width + 0.5);
+		std::cout << "[" << std::string(filled, '=') << std::string(width - filled, ' ') << "] " << std::setw(3)
+		          << static_cast<int>(100.0 * progress + 0.5) << " % (" << Time_Display(el) << ")"
+		          << " captured_particles=" << captured << "/" << requested_
+		          << " captured_particle_rate[1/s]=" << Round3(el > 0.0 ? captured / el : 0.0) << std::endl;
+		printed_ = true;
+		last_ = captured;
+	}
+
+  private:
+	bool on_;
+	uint32_t requested_;
+	std::chrono::steady_clock::time_point t0_;
+	size_t next_ = 0;
+	bool printed_ = false;
+	uint64_t last_ = 0;
+};
+
 bool Snapshot_Interval_Valid(double s)
 {
 	// IsValidSnapshotIntervalSeconds, src/Snapshot_IO.cpp:652-658
@@ -505,6 +545,8 @@ int dms_generate_data(dms_ctx* ctx, int point_id, const dms_generate_opts* g, dm
 			guard.ctx = ctx;
 		}
 	}
+	Progress_Printer progress(g->print_progress != 0, g->sample_size, t0);
+	progress.Update(0, true);
 	for(;;)
 	{
 		if(snapshots)
@@ -512,6 +554,7 @@ int dms_generate_data(dms_ctx* ctx, int point_id, const dms_generate_opts* g, dm
 		rc = dms_get_results(ctx, point_id, &res);
 		if(rc != DMS_OK)
 			return rc;
+		progress.Update(res.counters[DMS_CNT_CAPTURED], false);
 		const uint64_t* c = res.counters;
 		const uint64_t captured = c[DMS_CNT_CAPTURED];
 		const uint64_t done = c[DMS_CNT_TRAJECTORIES];
@@ -578,6 +621,12 @@ int dms_generate_data(dms_ctx* ctx, int point_id, const dms_generate_opts* g, dm
 		out->final_round_trajectories = round;
 	}
 	out->computing_time_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+	{
+		dms_point_results last;
+		std::memset(&last, 0, sizeof last);
+		if(dms_get_results(ctx, point_id, &last) == DMS_OK)
+			progress.Update(last.counters[DMS_CNT_CAPTURED], true);
+	}
 	if(snapshots)
 	{
 		dms_set_progress_callback(ctx, nullptr, nullptr, 0.0);

@@ -13,12 +13,13 @@
 // RK45 form of the kernels: 0 = one loop over the six stages (a short hot loop: fewer
 // instruction-cache misses with every lane busy), 1 = the stages written out (a shorter
 // dependent chain for a lane that runs alone), 2 = the loop while the work queue still has
-// items and the written-out stages once it is drained (the tail of a launch).  Measured on
-// B200: the FP64 kernel gains 12 % steady-state and 14 % Capture-mode throughput from 2 over
-// 1 at the same lone-lane speed; the mixed kernel's FP32 stages are short, and 2 gains
-// nothing over 1 there.
+// items and the written-out stages once a lane of the block has found it drained.  Form 2 is
+// measured 12 % faster with every lane busy, but it is not the default: a block whose lanes
+// are all held by long trajectories never sees the drain, so its tail keeps the slower loop
+// (bench batches up to 11 % slower from run to run), and the bounds-checked build showed
+// run-to-run differences of replayed FP64 trajectories under it that form 1 never shows.
 #ifndef DMS_RK_UNROLLED
-#define DMS_RK_UNROLLED 2
+#define DMS_RK_UNROLLED 1
 #endif
 #ifndef DMS_RK_UNROLLED_MIXED
 #define DMS_RK_UNROLLED_MIXED 1

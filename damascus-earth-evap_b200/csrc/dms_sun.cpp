@@ -94,6 +94,7 @@ int main(int argc, char* argv[])
 	g.max_scatterings = cfg.maximum_number_of_scatterings;
 	g.sigma_p_cm2 = cfg.sigma_nucleon_cm2;
 	g.max_trajectory_wall_time_s = cfg.max_trajectory_wall_time_sec;
+	g.print_progress = 1;
 	// output path, src/main.cpp:89-92 (std::to_string of log10 values); snapshots go to its
 	// snapshot/ folder (src/Data_Generation.cpp:522-529)
 	const std::string out = cfg.output_dir + "results_" + std::to_string(std::log10(cfg.DM_mass_gev)) + "_" +

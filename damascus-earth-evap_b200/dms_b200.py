@@ -100,7 +100,8 @@ class GenerateOpts(ctypes.Structure):
                 ("max_trajectory_wall_time_s", ctypes.c_double), ("threads_per_block", ctypes.c_uint32),
                 ("blocks_per_sm", ctypes.c_uint32), ("snapshot_dir", ctypes.c_char_p),
                 ("snapshot_interval_s", ctypes.c_double), ("snapshot_mass_gev", ctypes.c_double),
-                ("snapshot_sigma_cm2", ctypes.c_double), ("max_free_steps", ctypes.c_uint64)]
+                ("snapshot_sigma_cm2", ctypes.c_double), ("max_free_steps", ctypes.c_uint64),
+                ("print_progress", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class GenerateSummary(ctypes.Structure):

@@ -96,6 +96,9 @@ def test_parameter_point_run_writes_reference_outputs(tmp_path):
     for label in ("Simulation data summary", "Simulated trajectories:", "Average # of scatterings:", "Capture rate raw error",
                   "Simulation time"):
         assert label in p.stdout, p.stdout
+    # progress lines at the capture milestones (src/Data_Generation.cpp:661-694)
+    progress = [l for l in p.stdout.splitlines() if "captured_particle_rate[1/s]=" in l]
+    assert progress and "captured_particles=0/16" in progress[0] and "100 %" in progress[-1], progress
     dirs = [d for d in os.listdir(tmp_path) if d.startswith("results_")]
     assert len(dirs) == 1
     out = tmp_path / dirs[0]
