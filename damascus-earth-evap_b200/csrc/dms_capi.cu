@@ -1040,6 +1040,8 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 	int rc = Check_Run_Opts(ctx, opts);
 	if(rc != DMS_OK)
 		return rc;
+	if(!(opts->max_trajectory_wall_time_s >= 0.0) || !std::isfinite(opts->max_trajectory_wall_time_s))
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "'max_trajectory_wall_time_sec' must be finite and non-negative");
 	if(point_id < 0 || point_id >= static_cast<int>(ctx->points.size()))
 		return Fail(ctx, DMS_ERR_NO_POINT, "no such point");
 	if(count > DMS_NOALLOC_MAX_TRAJECTORIES)
@@ -1078,6 +1080,9 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 	p.max_free_steps = opts->max_free_steps;
 	p.boundary = opts->boundary_radius_rsun * DMS_RSUN_KM;
 	p.iteration_budget = opts->iteration_budget ? opts->iteration_budget : ~0ULL;
+	p.wall_limit_ns = static_cast<uint64_t>(opts->max_trajectory_wall_time_s * 1.0e9);
+	if(opts->max_trajectory_wall_time_s > 0.0 && p.wall_limit_ns == 0)
+		p.wall_limit_ns = 1;
 	p.ic_max_attempts = 1 << 20;
 	p.counters = ctx->d_counters;
 	p.hists = ctx->d_hists;

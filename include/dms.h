@@ -234,7 +234,8 @@ int dms_run_records(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64
  * DMS_NOALLOC_MAX_TRAJECTORIES trajectories fit one
  * call; larger counts return DMS_ERR_INVALID_ARGUMENT.  The FP64 kernel runs whatever
  * opts->precision says, with one lane per trajectory (threads_per_block and blocks_per_sm are
- * ignored).  The first call on a device looks the array up; make that call before any stream
+ * ignored); the other options, the per-trajectory wall-time limit included, apply as in
+ * dms_run_records.  The first call on a device looks the array up; make that call before any stream
  * capture on that device starts.  Every call on a device shares the array: calls that overlap
  * on the GPU (two contexts or two host threads on one device) race. */
 #define DMS_NOALLOC_MAX_TRAJECTORIES 128

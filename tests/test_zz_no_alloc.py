@@ -73,3 +73,6 @@ def test_noalloc_rejects_oversize_and_accepts_empty(engine):
     assert rc == -1  # DMS_ERR_INVALID_ARGUMENT
     assert "at most %d" % MAX_TRAJECTORIES in e.lib.dms_last_error(e.h).decode()
     assert e.lib.dms_run_records_noalloc(e.h, ctypes.byref(opts), pid, 0, 0, None, None, None) == 0
+    bad = dms_b200.run_opts(seed=7, max_trajectory_wall_time_s=-1.0)
+    assert e.lib.dms_run_records_noalloc(e.h, ctypes.byref(bad), pid, 0, 4, None, None, None) == -1
+    assert "max_trajectory_wall_time_sec" in e.lib.dms_last_error(e.h).decode()
