@@ -421,11 +421,6 @@ class Snapshot_Writer
 	std::vector<dms_evaporation_event> events_;
 };
 
-int Snapshot_Hook(dms_ctx*, void* user)
-{
-	static_cast<Snapshot_Writer*>(user)->Tick();
-	return 0;
-}
 
 // Removes the progress hook when the generate call returns, on every path.
 struct Hook_Guard
@@ -477,6 +472,30 @@ class Progress_Printer
 	bool printed_ = false;
 	uint64_t last_ = 0;
 };
+
+// What the driver does while a launch is in flight: snapshot reports that fall due, and the
+// progress lines of captures reached (read with dms_peek_results beside the kernel).
+struct Launch_Hook
+{
+	Snapshot_Writer* snapshots;
+	Progress_Printer* progress;
+	int point;
+};
+
+int Launch_Hook_Call(dms_ctx* ctx, void* user)
+{
+	const Launch_Hook& h = *static_cast<Launch_Hook*>(user);
+	if(h.snapshots)
+		h.snapshots->Tick();
+	if(h.progress)
+	{
+		dms_point_results r;
+		std::memset(&r, 0, sizeof r);
+		if(dms_peek_results(ctx, h.point, &r) == DMS_OK)
+			h.progress->Update(r.counters[DMS_CNT_CAPTURED], false);
+	}
+	return 0;
+}
 
 bool Snapshot_Interval_Valid(double s)
 {
@@ -537,16 +556,20 @@ int dms_generate_data(dms_ctx* ctx, int point_id, const dms_generate_opts* g, dm
 		if(!Snapshot_Interval_Valid(g->snapshot_interval_s))
 			return DMS_ERR_INVALID_ARGUMENT;
 		snapshots.reset(new Snapshot_Writer(ctx, point_id, *g, t0));
-		if(snapshots->ok())
-		{
-			rc = dms_set_progress_callback(ctx, Snapshot_Hook, snapshots.get(), std::min(0.1, 0.1 * g->snapshot_interval_s));
-			if(rc != DMS_OK)
-				return rc;
-			guard.ctx = ctx;
-		}
+		if(!snapshots->ok())
+			snapshots.reset();
 	}
 	Progress_Printer progress(g->print_progress != 0, g->sample_size, t0);
 	progress.Update(0, true);
+	Launch_Hook hook{snapshots.get(), g->print_progress ? &progress : nullptr, point_id};
+	if(hook.snapshots || hook.progress)
+	{
+		const double interval = hook.snapshots ? std::min(0.1, 0.1 * g->snapshot_interval_s) : 0.25;
+		rc = dms_set_progress_callback(ctx, Launch_Hook_Call, &hook, interval);
+		if(rc != DMS_OK)
+			return rc;
+		guard.ctx = ctx;
+	}
 	for(;;)
 	{
 		if(snapshots)
