@@ -16,8 +16,7 @@
 // items and the written-out stages once a lane of the block has found it drained.  Form 2 is
 // measured 12 % faster with every lane busy, but it is not the default: a block whose lanes
 // are all held by long trajectories never sees the drain, so its tail keeps the slower loop
-// (bench batches up to 11 % slower from run to run), and the bounds-checked build showed
-// run-to-run differences of replayed FP64 trajectories under it that form 1 never shows.
+// (bench batches up to 11 % slower from run to run).
 #ifndef DMS_RK_UNROLLED
 #define DMS_RK_UNROLLED 1
 #endif

@@ -465,13 +465,12 @@ __device__ __noinline__ void finalize(const RunParams& R, const DevPoint* __rest
 	}
 }
 
-// Moves the histogram rows of every lane of the converged group that terminated in this
-// iteration: all lanes of the group stride over one row at a time, so the row is read, the
+// Moves the histogram rows of every lane of the group `grp` (the whole warp) that terminated in
+// this iteration: all lanes of the group stride over one row at a time, so the row is read, the
 // per-point sums are updated and the row is zeroed with coalesced accesses instead of one
 // lane walking up to 2000 bins while the rest of its warp waits.
-__device__ __forceinline__ void cooperative_flush(double2* hist, FlushJob& job)
+__device__ __forceinline__ void cooperative_flush(double2* hist, FlushJob& job, unsigned int grp)
 {
-	const unsigned int grp = __activemask();
 	unsigned int pending = __ballot_sync(grp, job.b1 >= job.b0);
 	if(pending == 0u)
 		return;
@@ -577,16 +576,16 @@ __device__ __forceinline__ int start_trajectory(const RunParams& R, Lane& L, uin
 	return PH_SEGMENT;
 }
 
-// Sample_Target for every lane of the converged group that is at a scattering point.  The 64
+// Sample_Target for every lane of the group `grp` (the whole warp) at a scattering point.  The 64
 // channel rates of one scattering lane (63 isotopes + electrons, the dominant cost of a
 // scatter) are evaluated by all lanes of the group in parallel into shared memory; the
 // scattering lane then validates, sums and picks sequentially in the reference's order, so
 // the target and the draws consumed are those of the one-lane form.  `rates` is this warp's
 // DMS_NUM_TARGETS + 1 doubles of shared memory.
 template <class Lane, class Step>
-__device__ __forceinline__ void cooperative_targets(const RunParams& R, Lane& L, int phase, double* rates, int& target, const Step& step)
+__device__ __forceinline__ void cooperative_targets(const RunParams& R, Lane& L, int phase, double* rates, int& target, const Step& step,
+                                                    unsigned int grp)
 {
-	const unsigned int grp = __activemask();
 	unsigned int pending = __ballot_sync(grp, phase == PH_SCATTER);
 	if(pending == 0u)
 		return;
@@ -702,11 +701,19 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	int scatter_wait = 0;
 	int final_wait = 0;
 	const unsigned int lane_bit = 1u << (threadIdx.x & 31);
+	// Every lane stays in the loop until its whole warp is done (a lane without work waits in
+	// PH_DONE), and leaves only together with the others.  So the warp's collective steps
+	// below (batching votes, cooperative target sampling into the warp's shared rates, the
+	// histogram flush) always run with all 32 lanes, a fixed mask, instead of whichever lanes
+	// happen to be converged at that point.
+	constexpr unsigned int FULL_WARP = 0xffffffffu;
 	for(uint64_t iter = 0;; iter++)
 	{
+		if(__all_sync(FULL_WARP, phase == PH_DONE))
+			break;
 		if((iter & 1023) == 1023)
 		{
-			if(*R.cancel != 0)
+			if(__any_sync(FULL_WARP, *R.cancel != 0))
 			{
 				atomicOr(R.status, STATUS_CANCELLED);
 				break;
@@ -731,9 +738,10 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 			if(w >= R.total)
 			{
 				*reinterpret_cast<volatile int*>(&queue_drained) = 1;
-				break;
+				phase = PH_DONE;
 			}
-			phase = start_trajectory(R, L, w, P, m_dm);
+			else
+				phase = start_trajectory(R, L, w, P, m_dm);
 		}
 		if(phase == PH_SEGMENT)
 			phase = segment_start(R, P, m_dm, L);
@@ -743,7 +751,7 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 		// DMS_SCATTER_MAX_WAIT iterations, or no lane is stepping), so that the scattering code
 		// runs for many lanes at once.  A lane's draws do not depend on when it scatters.
 		{
-			const unsigned int grp = __activemask();
+			const unsigned int grp = FULL_WARP;
 			const unsigned int waiting = __ballot_sync(grp, phase == PH_SCATTER);
 			if(waiting != 0u)
 			{
@@ -753,7 +761,7 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 				if(go)
 				{
 					int target = TARGET_FAILED;
-					cooperative_targets(R, L, phase, rates, target, step);
+					cooperative_targets(R, L, phase, rates, target, step, grp);
 					if(phase == PH_SCATTER)
 					{
 						phase = finish_scatter(R, P, m_dm, L, target, step);
@@ -766,7 +774,7 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 		}
 		// terminations are batched the same way
 		{
-			const unsigned int grp = __activemask();
+			const unsigned int grp = FULL_WARP;
 			const unsigned int ending = __ballot_sync(grp, phase == PH_FINAL);
 			if(ending != 0u)
 			{
@@ -782,16 +790,17 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 						phase = PH_FETCH;
 						final_wait = 0;
 					}
-					cooperative_flush(hist, job);
+					cooperative_flush(hist, job, grp);
 				}
 				else if(phase == PH_FINAL)
 					final_wait++;
 			}
 		}
 	}
-	if(phase != PH_FETCH && L.bmax >= L.bmin)
+	const bool in_trajectory = phase != PH_FETCH && phase != PH_DONE;
+	if(in_trajectory && L.bmax >= L.bmin)
 		for(int b = L.bmin; b <= L.bmax; b++) hist[b] = make_double2(0.0, 0.0);
-	if(phase != PH_FETCH && R.records == nullptr)
+	if(in_trajectory && R.records == nullptr)
 	{
 		// stopped in mid-trajectory: count the work done so far
 		unsigned long long* c = R.counters + static_cast<size_t>(L.point) * DMS_NUM_COUNTERS;
