@@ -13,10 +13,10 @@
 // RK45 form of the kernels: 0 = one loop over the six stages (a short hot loop: fewer
 // instruction-cache misses with every lane busy), 1 = the stages written out (a shorter
 // dependent chain for a lane that runs alone), 2 = the loop while the work queue still has
-// items and the written-out stages once a lane of the block has found it drained.  Form 2 is
-// measured 12 % faster with every lane busy, but it is not the default: a block whose lanes
-// are all held by long trajectories never sees the drain, so its tail keeps the slower loop
-// (bench batches up to 11 % slower from run to run).
+// items and the written-out stages once the block has seen it drained (a lane's fetch, or the
+// queue head read every 64 iterations).  Form 2 is measured 10 % faster with every lane busy
+// and 8 % faster in Capture mode; the default stays 1 because the bench step is bounded by its
+// tail, which form 2 does not shorten.
 #ifndef DMS_RK_UNROLLED
 #define DMS_RK_UNROLLED 1
 #endif

@@ -711,6 +711,13 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	{
 		if(__all_sync(FULL_WARP, phase == PH_DONE))
 			break;
+#if DMS_RK_UNROLLED == 2 || DMS_RK_UNROLLED_MIXED == 2
+		// a block whose lanes are all held by long trajectories learns of the drained queue from
+		// the queue head itself (one read per warp every 64 iterations)
+		if((iter & 63) == 63 && (threadIdx.x & 31) == 0 &&
+		   *reinterpret_cast<volatile unsigned long long*>(R.queue_head) >= R.total)
+			*reinterpret_cast<volatile int*>(&queue_drained) = 1;
+#endif
 		if((iter & 1023) == 1023)
 		{
 			if(__any_sync(FULL_WARP, *R.cancel != 0))
