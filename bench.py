@@ -52,6 +52,21 @@ FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ = 214.8, 622.3,
 TRAFFIC_PER_TRAJECTORY = (2524931584 + 3947619584) / 65536
 
 
+def hbm_peak_gbs():
+    """The measured HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json, written next to
+    this file by the machine's set-up), else the earlier measurement 6650 GB/s."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            peaks = json.load(f)
+        for key in ("hbm_gbs", "hbm_GBs", "hbm"):
+            if key in peaks and isinstance(peaks[key], (int, float)):
+                return float(peaks[key]), "measured (MEASURED_PEAKS.json %s)" % key
+    except (OSError, ValueError):
+        pass
+    return 6650.0, "fallback 6.65 TB/s (no measured peak file)"
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -372,6 +387,12 @@ def run_engine_arm(args):
                              FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ)},
             "clocks": clock_info,
         }
+        # the memory view of the same launch: its DRAM bytes over its time against the HBM copy
+        # bandwidth, which shows that the kernel is not memory-bound
+        hbm_peak, hbm_source = hbm_peak_gbs()
+        hbm_achieved = line["roofline"]["traffic"] / (dev_ms * 1e-3) / 1e9
+        line["roofline"]["hbm"] = {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                                   "frac": hbm_achieved / hbm_peak, "peak_source": hbm_source}
         if steady:
             line["steady_state"] = steady
         if not args.no_mixed:
