@@ -58,7 +58,9 @@ typedef struct
 	uint64_t max_free_steps;     /* maximum_free_time_steps of Configure; 0 = the default (1e12) */
 	int32_t print_progress;      /* 1: progress lines on stdout at 0, 1, 5, 10, 20, 40, 60, 80 and 100 % of
 	                                the captures, checked while launches run and after each
-	                                (src/Data_Generation.cpp:661-694) */
+	                                (src/Data_Generation.cpp:661-694).  With snapshots or progress
+	                                lines on, dms_generate_data uses the context's progress hook
+	                                (dms_set_progress_callback) and removes it when it returns. */
 	int32_t reserved;
 } dms_generate_opts;
 
