@@ -72,6 +72,10 @@ class EvaporationEvent(ctypes.Structure):
     _fields_ = [("trajectory_id", ctypes.c_uint64), ("lifetime_unbinding", ctypes.c_double)]
 
 
+# numpy view of dms_evaporation_event
+EVENT_DTYPE = np.dtype([("trajectory_id", np.uint64), ("lifetime_unbinding", np.float64)])
+
+
 class Reflection(ctypes.Structure):
     _fields_ = [("trajectory_id", ctypes.c_uint64), ("speed_kms", ctypes.c_double), ("cos_sun_velocity", ctypes.c_double)]
 
@@ -320,20 +324,18 @@ class Engine:
     def _results(self, getter, point, events_capacity, reflections_capacity):
         res = PointResults()
         hist = np.zeros(NUM_HISTS * NUM_BINS)
-        events = (EvaporationEvent * events_capacity)()
+        events = np.empty(events_capacity, dtype=EVENT_DTYPE)
         refl = np.zeros(reflections_capacity, dtype=[("trajectory_id", np.uint64), ("speed_kms", np.float64),
                                                       ("cos_sun_velocity", np.float64)])
         res.histograms = hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-        res.events = events
+        res.events = events.ctypes.data_as(ctypes.POINTER(EvaporationEvent))
         res.events_capacity = events_capacity
         res.reflections = refl.ctypes.data_as(ctypes.POINTER(Reflection))
         res.reflections_capacity = reflections_capacity
         self._check(getter(self.h, point, ctypes.byref(res)))
         counters = {name: int(res.counters[k]) for k, name in COUNTER_NAMES.items()}
         counters["reasons"] = [int(res.counters[REASON_BASE + k]) for k in range(11)]
-        n = min(res.events_count, events_capacity)
-        ev = np.array([(events[i].trajectory_id, events[i].lifetime_unbinding) for i in range(n)],
-                      dtype=[("trajectory_id", np.uint64), ("lifetime_unbinding", np.float64)])
+        ev = events[:min(res.events_count, events_capacity)].copy()
         out = {"counters": counters, "histograms": hist.reshape(NUM_HISTS, NUM_BINS), "events": ev,
                "reflections_count": int(res.reflections_count)}
         if reflections_capacity:
