@@ -964,7 +964,7 @@ int dms_peek_results(dms_ctx* ctx, int point_id, dms_point_results* r)
 // budget before any work arrives and must not fail on an allocation later.  For them this
 // entry point writes into the caller's device buffers and keeps its scratch in the array
 // below, which is part of the library's device image: every device that loads the library
-// holds these 4 MiB until the process exits.
+// holds these DMS_NOALLOC_SCRATCH_BYTES (4 104 448 bytes, about 3.9 MiB) until the process exits.
 //
 // Scratch layout (bytes): 0 work-queue head (u64), 8 status word (u32), 64 range start (u64),
 // 72 range offsets {0, count} (2 x u64), 96 range point (i32); from 256 the initial states
@@ -983,7 +983,9 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
 
-// Address of the scratch array on the context's device (current), looked up once per device.
+// Address of the scratch array on the context's device (current), looked up once per device
+// and kept for the life of the process.  A device reset (cudaDeviceReset) between calls would
+// leave the kept address stale; the header states that such a reset is not supported.
 int Noalloc_Scratch(dms_ctx* ctx, unsigned char** out)
 {
 	if(ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES)
@@ -1037,6 +1039,9 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 {
 	if(!ctx)
 		return DMS_ERR_INVALID_ARGUMENT;
+	// from a progress callback this would clear the outer launch's cancel flag, re-record its
+	// timing events and block the outer wait loop behind the running kernel
+	DMS_NOT_IN_FLIGHT(ctx);
 	int rc = Check_Run_Opts(ctx, opts);
 	if(rc != DMS_OK)
 		return rc;
@@ -1096,6 +1101,9 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 	p.rec_hist_v2dt = d_hist_v2dt;
 	p.cancel = ctx->d_cancel;
 
+#ifdef DMS_CHECKED
+	(void)Take_Bounds_Status();   // bits of an earlier launch are not this call's
+#endif
 	*ctx->h_cancel = 0;
 	noalloc_prepare_kernel<<<8, 256, 0, ctx->stream>>>(scratch, first, count, point_id, lanes, reinterpret_cast<unsigned char*>(d_records),
 	                                                   d_hist_dt, d_hist_v2dt);
@@ -1134,6 +1142,11 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 		return Fail(ctx, DMS_ERR_BUDGET, "run stopped: per-lane iteration budget exhausted");
 	if(status & STATUS_IC_REJECTION)
 		ctx->error = "warning: an initial-condition rejection loop hit its attempt bound";
+#ifdef DMS_CHECKED
+	const unsigned int bounds = Take_Bounds_Status();
+	if(bounds != 0)
+		return Fail(ctx, DMS_ERR_STATE, "checked build: an index left its bounds (bits " + std::to_string(bounds) + ")");
+#endif
 	return DMS_OK;
 }
 

@@ -163,6 +163,7 @@ def library():
     lib.dms_default_run_opts.restype = None
     lib.dms_run.argtypes = [vp, c.POINTER(RunOpts), c.POINTER(WorkRange), c.c_int]
     lib.dms_run_records.argtypes = [vp, c.POINTER(RunOpts), c.c_int, c.c_uint64, c.c_uint64, c.POINTER(TrajRecord), vp, vp]
+    lib.dms_run_records_noalloc.argtypes = [vp, c.POINTER(RunOpts), c.c_int, c.c_uint64, c.c_uint64, vp, vp, vp]
     lib.dms_get_results.argtypes = [vp, c.c_int, c.POINTER(PointResults)]
     lib.dms_reset_results.argtypes = [vp, c.c_int]
     lib.dms_num_bins.restype = c.c_int
@@ -286,6 +287,13 @@ class Engine:
         if histograms:
             out["hist_dt"], out["hist_v2dt"] = hd, hv
         return out
+
+    def run_records_noalloc(self, point, first, count, opts, d_records, d_hist_dt=None, d_hist_v2dt=None):
+        """dms_run_records_noalloc: the same records written into caller-owned DEVICE buffers
+        (integer device addresses, e.g. a torch tensor's data_ptr()); the library allocates
+        nothing for the call."""
+        self._check(self.lib.dms_run_records_noalloc(self.h, ctypes.byref(opts), point, first, count, d_records,
+                                                     d_hist_dt, d_hist_v2dt))
 
     def results(self, point, events_capacity=1 << 20, reflections_capacity=0):
         """Accumulated results of a point (dms_get_results)."""

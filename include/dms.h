@@ -232,12 +232,15 @@ int dms_run_records(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64
  * word, initial states, one 2000-bin histogram row per lane) is a fixed array of
  * DMS_NOALLOC_SCRATCH_BYTES in the library's device image, so at most
  * DMS_NOALLOC_MAX_TRAJECTORIES trajectories fit one
- * call; larger counts return DMS_ERR_INVALID_ARGUMENT.  The FP64 kernel runs whatever
- * opts->precision says, with one lane per trajectory (threads_per_block and blocks_per_sm are
- * ignored); the other options, the per-trajectory wall-time limit included, apply as in
- * dms_run_records.  The first call on a device looks the array up; make that call before any stream
- * capture on that device starts.  Every call on a device shares the array: calls that overlap
- * on the GPU (two contexts or two host threads on one device) race. */
+ * call; larger counts return DMS_ERR_INVALID_ARGUMENT.  It always runs the FP64 kernel:
+ * opts->precision is ignored (MIXED runs FP64 too), and so are threads_per_block and
+ * blocks_per_sm (one lane per trajectory); the other options, the per-trajectory wall-time
+ * limit included, apply as in dms_run_records.  Like the other launching calls it is refused
+ * (DMS_ERR_STATE) from a progress callback.  The first call on a device looks the array up
+ * and keeps its address for the life of the process; make that call before any stream capture
+ * on that device starts, and do not reset the device (cudaDeviceReset) between calls.  Every
+ * call on a device shares the array: calls that overlap on the GPU (two contexts or two host
+ * threads on one device) race.  DMS_NOALLOC_SCRATCH_BYTES is 4 104 448 bytes (about 3.9 MiB). */
 #define DMS_NOALLOC_MAX_TRAJECTORIES 128
 #define DMS_NOALLOC_SCRATCH_BYTES    (256 + DMS_NOALLOC_MAX_TRAJECTORIES * (64 + 2000 * 16))
 int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64_t first, uint64_t count,

@@ -2,7 +2,7 @@
 #ifndef DMS_SHIM_VERSION_HPP
 #define DMS_SHIM_VERSION_HPP
 #ifndef DMS_REFERENCE_DIR
-#define DMS_REFERENCE_DIR "/root/reference"
+#error "DMS_REFERENCE_DIR (the data directory of the reference build) must be defined by the build"
 #endif
 #define PROJECT_DIR DMS_REFERENCE_DIR
 #define PROJECT_NAME "DaMaSCUS-SUN"

@@ -1,8 +1,8 @@
 """The bounds-checked build (libdms_cuda_checked.so, -DDMS_CHECKED): every solar-table knot,
 rate-grid cell, histogram bin and row, work range and scattering target index is tested on
 the device, and a launch that saw one out of bounds fails with DMS_ERR_STATE.  Both kernels run
-the replay, direct-rate, dark-photon and ragged-launch workloads under it; the FP64 records must
-still equal the oracle's (B200 required).  The library is loaded in a child process, since one
+the replay, direct-rate, dark-photon and ragged-launch workloads under it, and so does the
+no-alloc entry point; the FP64 records must still equal the oracle's (B200 required).  The library is loaded in a child process, since one
 process holds one engine library."""
 import os
 import subprocess
@@ -47,6 +47,14 @@ with dms_b200.Engine(0) as e:
                   dms_b200.run_opts(seed=3, capture_mode=capture, max_scatterings=10 ** 5, time_limit_s=120.0,
                                     precision=prec))
             assert e.results(pid, events_capacity=1)["counters"]["trajectories"] == 734
+        if n_grid and not capture:
+            import ctypes, torch
+            d_rec = torch.zeros(ctypes.sizeof(dms_b200.TrajRecord) * 96, dtype=torch.uint8, device="cuda:0")
+            d_hd = torch.zeros((96, dms_b200.NUM_BINS), dtype=torch.float64, device="cuda:0")
+            d_hv = torch.zeros_like(d_hd)
+            e.run_records_noalloc(pid, 3000, 96, opts, d_rec.data_ptr(), d_hd.data_ptr(), d_hv.data_ptr())
+            torch.cuda.synchronize()
+            assert d_rec.cpu().numpy().tobytes() == bytes(e.run_records(pid, 3000, 96, opts)["records"])
 print("checked build: no index out of bounds")
 '''
 

@@ -72,7 +72,8 @@ def test_calls_that_change_the_launch_are_refused_in_the_hook(engine):
     def hook(eng):
         for call in (lambda: eng.add_point(dms_b200.point_params(0.3, 1e-36, interpolation_points=50)),
                      lambda: eng.reset_results(pid),
-                     lambda: eng.run([(pid, 0, 4)], dms_b200.run_opts(seed=1))):
+                     lambda: eng.run([(pid, 0, 4)], dms_b200.run_opts(seed=1)),
+                     lambda: eng.run_records_noalloc(pid, 0, 4, dms_b200.run_opts(seed=1), None)):
             try:
                 call()
             except dms_b200.EngineError as err:
@@ -85,7 +86,7 @@ def test_calls_that_change_the_launch_are_refused_in_the_hook(engine):
             e.run([(pid, 0, QUEUE)], dms_b200.run_opts(seed=3, max_scatterings=10 ** 6, time_limit_s=60.0))
     finally:
         e.set_progress_callback(None)
-    assert refused == [True, True, True]
+    assert refused == [True, True, True, True]
     n = e.lib.dms_num_points(e.h)
     assert n == 1   # the refused add_point left no point behind
 
