@@ -2082,6 +2082,19 @@ int dms_oracle_rate_grid(const dms_oracle* o, double* grid)
 	return DMS_OK;
 }
 
+/* Replaces the current point's N x N grid (the rate_grid member of Solar_Model,
+ * include/Solar_Model.hpp:309) by one built elsewhere: the test of the engine's own device-built
+ * grid replays the oracle on that grid, the same role dms_set_rate_grid plays for the engine. */
+int dms_oracle_set_rate_grid(dms_oracle* o, const double* grid, uint32_t n)
+{
+	if(!o || !o->has_point)
+		return DMS_ERR_NO_POINT;
+	if(!grid || n < 2 || (int)n != o->grid_n)
+		return DMS_ERR_INVALID_ARGUMENT;
+	memcpy(o->grid, grid, (size_t)n * n * sizeof(double));
+	return DMS_OK;
+}
+
 int dms_oracle_run_records(dms_oracle* o, uint32_t seed, uint32_t point, int capture_mode, uint64_t max_scatterings,
                            double boundary_rsun, uint64_t first, uint64_t count, dms_traj_record* records, double* hist_dt,
                            double* hist_v2dt, double* trace, size_t trace_capacity, size_t* trace_length)

@@ -39,6 +39,8 @@ int dms_oracle_tables(const dms_oracle* o, double* r, double* gm, double* temper
 int dms_oracle_num_nodes(const dms_oracle* o);
 /* Rate grid of the current point (N*N doubles, radius-major, 1/s). */
 int dms_oracle_rate_grid(const dms_oracle* o, double* grid);
+/* Replaces the current point's grid by n*n values (n must equal its interpolation_points). */
+int dms_oracle_set_rate_grid(dms_oracle* o, const double* grid, uint32_t n);
 
 int dms_oracle_run_records(dms_oracle* o, uint32_t seed, uint32_t point, int capture_mode, uint64_t max_scatterings,
                            double boundary_rsun, uint64_t first, uint64_t count, dms_traj_record* records, double* hist_dt,

@@ -85,6 +85,7 @@ class Oracle:
         lib.dms_oracle_num_nodes.argtypes = [ctypes.c_void_p]
         lib.dms_oracle_tables.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 6
         lib.dms_oracle_rate_grid.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.dms_oracle_set_rate_grid.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]
         lib.dms_oracle_run_records.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
                                                ctypes.c_uint64, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64,
                                                ctypes.POINTER(TrajRecord), ctypes.c_void_p, ctypes.c_void_p,
@@ -125,6 +126,14 @@ class Oracle:
         g = np.zeros(self.point_n * self.point_n)
         self.lib.dms_oracle_rate_grid(self.h, g.ctypes.data)
         return g.reshape(self.point_n, self.point_n)
+
+    def set_rate_grid(self, grid):
+        """Replays on a grid built elsewhere (e.g. the engine's device-built grid)."""
+        import numpy as np
+        g = np.ascontiguousarray(grid, dtype=np.float64).reshape(-1)
+        rc = self.lib.dms_oracle_set_rate_grid(self.h, g.ctypes.data, self.point_n)
+        if rc != 0:
+            raise RuntimeError("oracle set_rate_grid failed %d" % rc)
 
     def run_records(self, seed, point, first, count, capture_mode=False, max_scatterings=10**6, boundary_rsun=2.0,
                     histograms=False, trace_capacity=0):

@@ -1,0 +1,104 @@
+"""The FP64 engine against the reference's own CPU run of the same configuration: the
+reference's sources (oracle/_ref, compiled unmodified against the shims) run the same
+trajectory ids on every host core, and the engine runs them on the B200 with its own
+device-built 1000 x 1000 rate grid (B200 and the reference build required).
+
+Per configuration, as the ensemble oracle asks:
+* the capture fraction within one binomial standard error of the reference's;
+* the radial histogram of captured particles (time-weighted dt, per trajectory) by per-bin
+  chi-squared, p > 0.05;
+* the evaporation-time distribution by a two-sample Kolmogorov-Smirnov test, p > 0.05;
+* every gate of the reference's validation/physics_validation.py:192-309 (capture intervals
+  overlap, evaporation fraction z <= 3, mean scatterings within 10 %, captured radial total
+  variation <= 0.10, evaporation median within 20 % and p90 within 30 %).
+Both runs draw from the same Philox streams, so most trajectories agree one by one; the
+fraction with identical scatter count, reason, flags and draw count is reported and must be at
+least 97 % (the rest part ways at the surface knife edge,
+src/Simulation_Trajectory.cpp:886-899, or through the last-bit differences of the grid's
+erf/exp and of the unit system, and then follow their own random walks).
+
+Workloads: the Parameter-point benchmark point (m = 0.3 GeV, sigma_n = 1e-36 cm^2, seed 7,
+max 1e6 scatterings, 65 536 ids: >= 8 192 captures, the run's sample size) and the Capture-mode
+benchmark point (m = 1 GeV, sigma_n = 1e-35 cm^2, seed 1, max 1e5 scatterings, 16 384 ids)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from dms_ctypes import REF_LIB
+from engine_fixtures import dms_b200
+import cpu_pool
+import dms_stats
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference build oracle/_ref not built")]
+
+CONFIGS = {
+    "parameter_point": dict(params=dict(mass_gev=0.3, sigma_p_cm2=1e-36, interpolation_points=1000), seed=7,
+                            capture_mode=False, max_scatterings=10 ** 6, count=1 << 16, min_captured=8192),
+    "capture": dict(params=dict(mass_gev=1.0, sigma_p_cm2=1e-35, interpolation_points=1000), seed=1,
+                    capture_mode=True, max_scatterings=10 ** 5, count=1 << 14, min_captured=1000),
+}
+
+
+@pytest.fixture(scope="module")
+def engine():
+    e = dms_b200.Engine(0)
+    yield e
+    e.close()
+
+
+def outcome_table(records, count):
+    out = np.zeros(count, dtype=cpu_pool.OUTCOME_DTYPE)
+    for k in range(count):
+        r = records[k]
+        out[k] = (r.trajectory_id, r.number_of_scatterings, r.number_of_draws, r.termination_reason, r.flags,
+                  r.final_time, r.lifetime_unbinding,
+                  (r.final_time,) + tuple(r.final_position) + tuple(r.final_velocity))
+    return out
+
+
+def ks_pvalue(a, b):
+    from scipy.stats import ks_2samp
+    return float(ks_2samp(a, b).pvalue)
+
+
+@pytest.mark.parametrize("name", sorted(CONFIGS))
+def test_engine_ensemble_agrees_with_the_reference_run(engine, name):
+    cfg = CONFIGS[name]
+    p = cfg["params"]
+    n = cfg["count"]
+    pid = engine.add_point(dms_b200.point_params(p["mass_gev"], p["sigma_p_cm2"],
+                                                 interpolation_points=p["interpolation_points"]))
+    opts = dms_b200.run_opts(seed=cfg["seed"], capture_mode=cfg["capture_mode"], max_scatterings=cfg["max_scatterings"],
+                             time_limit_s=600.0)
+    engine.run([(pid, 0, n)], opts)
+    mine = engine.results(pid, events_capacity=1 << 17)
+    mine_out = outcome_table(engine.run_records(pid, 0, n, opts)["records"], n)
+    ref = cpu_pool.run_ensemble("reference", p, cfg["seed"], 0, n, capture_mode=cfg["capture_mode"],
+                                max_scatterings=cfg["max_scatterings"])
+    ro = ref["outcomes"]
+    same = ((mine_out["nscat"] == ro["nscat"]) & (mine_out["reason"] == ro["reason"]) &
+            (mine_out["flags"] == ro["flags"]) & (mine_out["draws"] == ro["draws"]))
+    cmp = dms_stats.compare_runs(ref, mine)
+    gates = dms_stats.reference_gates(ref, mine)
+    report = {"config": name, "trajectories": n, "identical_outcomes": float(same.mean()),
+              "differing_ids": [int(i) for i in ro["id"][~same][:20]],
+              "captured": [ref["counters"]["captured"], mine["counters"]["captured"]],
+              "capture_fraction_sigmas": cmp["capture_fraction_sigmas"],
+              "radial_chi2": cmp["radial_chi2"], "radial_dof": cmp["radial_dof"], "radial_p_value": cmp["radial_p_value"],
+              "gates": {k: [bool(ok), v] for k, (ok, v) in gates.items()}}
+    if not cfg["capture_mode"]:
+        report["events"] = [len(ref["events"]), len(mine["events"])]
+        report["evaporation_ks_p"] = ks_pvalue(ref["events"]["lifetime_unbinding"], mine["events"]["lifetime_unbinding"])
+    print(json.dumps(report, default=str))
+    assert mine["counters"]["trajectories"] == n
+    assert ref["counters"]["captured"] >= cfg["min_captured"], report
+    assert mine["counters"]["total_scatterings"] == int(mine_out["nscat"].sum())
+    assert cmp["capture_fraction_sigmas"] <= 1.0, report
+    assert not [k for k, (ok, _) in gates.items() if not ok], report
+    assert same.mean() >= 0.97, report
+    if not cfg["capture_mode"]:
+        assert cmp["radial_p_value"] > 0.05, report
+        assert len(ref["events"]) >= 1000 and report["evaporation_ks_p"] > 0.05, report
