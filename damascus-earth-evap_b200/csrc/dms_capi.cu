@@ -462,6 +462,29 @@ int dms_measure_fp64_peak(dms_ctx* ctx, double* tflops)
 	return DMS_OK;
 }
 
+int dms_check_certified_math(dms_ctx* ctx, uint64_t n, uint64_t seed, uint64_t* counts)
+{
+	if(!ctx || !counts)
+		return DMS_ERR_INVALID_ARGUMENT;
+	DMS_NOT_IN_FLIGHT(ctx);
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	unsigned long long* d = nullptr;
+	DMS_CUDA(ctx, cudaMalloc(&d, 4 * sizeof(unsigned long long)));
+	struct Free
+	{
+		void* p;
+		~Free() { cudaFree(p); }
+	} f{d};
+	DMS_CUDA(ctx, cudaMemsetAsync(d, 0, 4 * sizeof(unsigned long long), ctx->stream));
+	Check_Certified_Math(n, seed, d, ctx->sm_count, ctx->stream);
+	DMS_CUDA(ctx, cudaGetLastError());
+	unsigned long long h[4];
+	DMS_CUDA(ctx, cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+	DMS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+	for(int i = 0; i < 4; i++) counts[i] = h[i];
+	return DMS_OK;
+}
+
 int dms_last_kernel_ms(const dms_ctx* ctx, double* ms)
 {
 	if(!ctx || !ms)
@@ -512,6 +535,7 @@ int dms_load_solar_model(dms_ctx* ctx, const char* path)
 	DevSolar& S = ctx->dsolar;
 	S.n = t.n;
 	S.nbuckets = t.nbuckets;
+	S.bucket_single_step = t.bucket_single_step;
 	S.bucket_scale = static_cast<double>(t.nbuckets) / DMS_RSUN_KM;
 	S.r = dd + offsets[0];
 	S.gm = dd + offsets[1];

@@ -13,6 +13,7 @@
 #include "../../include/dms_math.h"
 #include "../../include/dms_nuclear_data.h"
 #include "../../include/dms_philox.h"
+#include "dms_fastmath.cuh"
 
 namespace dms
 {
@@ -56,6 +57,7 @@ struct DevSolar
 {
 	int n;                 // knots
 	int nbuckets;
+	int bucket_single_step;  // 1: the knot interval of x is its bucket's base or the base + 1
 	double bucket_scale;   // nbuckets / R_sun
 	const double* r;
 	const double* gm;
@@ -129,6 +131,17 @@ __device__ __forceinline__ double clamp_unit(double c) { return c < 0.0 ? 0.0 : 
 __device__ __forceinline__ int knot_index(const DevSolar& S, double x)
 {
 	const int last = S.n - 2;
+	if(S.bucket_single_step)
+	{
+		// one select, the same interval as the search below: x < 0 or NaN maps to bucket 0
+		// (base 0, no step up), x beyond the last knot to a base of last - 1 or last
+		const double xc = !(x >= 0.0) ? 0.0 : (x > DMS_RSUN_KM ? DMS_RSUN_KM : x);
+		int b = static_cast<int>(xc * S.bucket_scale);
+		b = b > S.nbuckets ? S.nbuckets : b;
+		int i = __ldg(S.bucket + b);
+		DMS_CHECK_INDEX(i, 0, last + 1, BOUNDS_KNOT);
+		return i + ((i < last) & (__ldg(S.r + i + 1) <= x));
+	}
 	if(x >= __ldg(S.r + last))
 		return last;
 	if(!(x >= 0.0))
@@ -151,6 +164,23 @@ __device__ __forceinline__ double table_eval(const DevSolar& S, const double* y,
 // Solar_Model::Mass (as G*M), src/Solar_Model.cpp:168-179
 __device__ __forceinline__ double solar_gm(const DevSolar& S, double r)
 {
+	if(S.bucket_single_step)
+	{
+		// without branches: both candidate intervals are loaded together with the bucket's
+		// base, and the same interval and arithmetic as below are selected
+		const double x = r < 0.0 ? 0.0 : r;
+		const double xc = !(x >= 0.0) ? 0.0 : (x > DMS_RSUN_KM ? DMS_RSUN_KM : x);
+		int b = static_cast<int>(xc * S.bucket_scale);
+		b = b > S.nbuckets ? S.nbuckets : b;
+		int i = __ldg(S.bucket + b);
+		DMS_CHECK_INDEX(i, 0, S.n - 1, BOUNDS_KNOT);
+		const double r0 = __ldg(S.r + i), r1 = __ldg(S.r + i + 1);
+		const double y0 = __ldg(S.gm + i), y1 = __ldg(S.gm + i + 1);
+		const double s0 = __ldg(S.gm_s + i), s1 = __ldg(S.gm_s + i + 1);
+		const bool up = (i < S.n - 2) & (r1 <= x);
+		const double v = up ? y1 + (x - r1) * s1 : y0 + (x - r0) * s0;
+		return !isfinite(r) ? NAN : (r > DMS_RSUN_KM ? DMS_GMSUN_KM3S2 : v);
+	}
 	if(!isfinite(r))
 		return NAN;
 	if(r < 0.0)
@@ -634,37 +664,111 @@ enum RkResult : int
 	RK_FORCED = 2,
 };
 
-// The same attempt with the six stages written out: a longer instruction stream (more
+// Arithmetic policies of the RK45 attempt: IEEE division and square root as written, or the
+// certified straight-line forms of dms_fastmath.cuh (bit-identical whenever `good` stays set;
+// the caller repeats the attempt with IeeeMath otherwise).
+struct IeeeMath
+{
+	struct Rcp
+	{
+		double b;
+	};
+	__device__ __forceinline__ Rcp rcp(double b) const { return Rcp{b}; }
+	__device__ __forceinline__ double div(double a, const Rcp& d) const { return a / d.b; }
+	__device__ __forceinline__ double div(double a, double b) const { return a / b; }
+	__device__ __forceinline__ double root(double x) const { return sqrt(x); }
+};
+
+struct CertMath
+{
+	bool good = true;
+	using Rcp = fast::Recip;
+	__device__ __forceinline__ Rcp rcp(double b) const { return fast::recip(b); }
+	__device__ __forceinline__ double div(double a, const Rcp& d) { return fast::div(a, d, good); }
+	__device__ __forceinline__ double div(double a, double b) { return fast::div(a, b, good); }
+	__device__ __forceinline__ double root(double x) { return fast::sqrt(x, good); }
+};
+
+// RK45_Next_Step_Size (src/Simulation_Trajectory.cpp:477-502) under an arithmetic policy;
+// pow(c, 0.25) is sqrt(sqrt(c)) as in dms_pow_quarter.
+template <class M>
+__device__ __forceinline__ double next_step_size_t(M& m, double current, double e0, double e1, double e2)
+{
+	if(!isfinite(e0) || !isfinite(e1) || !isfinite(e2))
+		return DMS_RK45_MIN_STEP_FACTOR * current;
+	double factor = DMS_RK45_MAX_STEP_FACTOR;
+	double c;
+	if(e0 > 0.0)
+	{
+		c = 0.84 * m.root(m.root(m.div(DMS_RK45_TOL_R_KM, e0)));
+		if(isfinite(c) && c < factor) factor = c;
+	}
+	if(e1 > 0.0)
+	{
+		c = 0.84 * m.root(m.root(m.div(DMS_RK45_TOL_V_KMS, e1)));
+		if(isfinite(c) && c < factor) factor = c;
+	}
+	if(e2 > 0.0)
+	{
+		c = 0.84 * m.root(m.root(m.div(DMS_RK45_TOL_PHI, e2)));
+		if(isfinite(c) && c < factor) factor = c;
+	}
+	if(factor > DMS_RK45_MAX_STEP_FACTOR) factor = DMS_RK45_MAX_STEP_FACTOR;
+	if(factor < DMS_RK45_MIN_STEP_FACTOR) factor = DMS_RK45_MIN_STEP_FACTOR;
+	return sanitized_step(factor * current);
+}
+
+// dv/dt and dphi/dt of one stage at radius r: J*J/r/r/r - gm/r/r with r clamped to >= 1 km, and
+// J/r/r (0 in radial mode, for J = 0 or r <= 0), the reference's divisions in its order.  The
+// quotients by the same r share one reciprocal under CertMath.
+template <class M>
+__device__ __forceinline__ void stage_rates(M& m, const Prop& p, double r, double gm, double& dv, double& dphi, bool want_phi)
+{
+	const double rc = r < 1.0 ? 1.0 : r;
+	const auto R = m.rcp(rc);
+	dv = m.div(m.div(m.div(p.J * p.J, R), R), R) - m.div(m.div(gm, R), R);
+	dphi = 0.0;
+	if(want_phi && !(p.radial_mode || p.J == 0.0 || r <= 0.0))
+		dphi = r < 1.0 ? m.div(m.div(p.J, r), r) : m.div(m.div(p.J, R), R);
+}
+
+// The attempt with the six stages written out: a longer instruction stream (more
 // instruction-cache pressure with many warps) but a shorter dependent chain for a lane that
 // runs alone.
-__device__ __forceinline__ int rk45_attempt_unrolled(const DevSolar& S, Prop& p, int inner)
+template <class M>
+__device__ __forceinline__ int rk45_attempt_t(const DevSolar& S, Prop& p, int inner, M& m)
 {
 	{
 		const double dt = p.time_step;
-		const double J = p.J;
-		double kr0, kr1, kr2, kr3, kr4, kr5, kv0, kv1, kv2, kv3, kv4, kv5, kp0, kp2, kp3, kp4, kp5, ri;
+		double kr0, kr1, kr2, kr3, kr4, kr5, kv0, kv1, kv2, kv3, kv4, kv5, kp0, kp2, kp3, kp4, kp5, ri, a, b;
 		kr0 = dt * p.v_radial;
-		kv0 = dt * dv_dt(J, p.radius, solar_gm(S, p.radius));
-		kp0 = dt * dphi_dt(p, p.radius);
+		stage_rates(m, p, p.radius, solar_gm(S, p.radius), a, b, true);
+		kv0 = dt * a;
+		kp0 = dt * b;
 		ri = p.radius + kr0 / 4.0;
 		kr1 = dt * (p.v_radial + kv0 / 4.0);
-		kv1 = dt * dv_dt(J, ri, solar_gm(S, ri));
+		stage_rates(m, p, ri, solar_gm(S, ri), a, b, false);
+		kv1 = dt * a;
 		ri = p.radius + 3.0 / 32.0 * kr0 + 9.0 / 32.0 * kr1;
 		kr2 = dt * (p.v_radial + 3.0 / 32.0 * kv0 + 9.0 / 32.0 * kv1);
-		kv2 = dt * dv_dt(J, ri, solar_gm(S, ri));
-		kp2 = dt * dphi_dt(p, ri);
+		stage_rates(m, p, ri, solar_gm(S, ri), a, b, true);
+		kv2 = dt * a;
+		kp2 = dt * b;
 		ri = p.radius + 1932.0 / 2197.0 * kr0 - 7200.0 / 2197.0 * kr1 + 7296.0 / 2197.0 * kr2;
 		kr3 = dt * (p.v_radial + 1932.0 / 2197.0 * kv0 - 7200.0 / 2197.0 * kv1 + 7296.0 / 2197.0 * kv2);
-		kv3 = dt * dv_dt(J, ri, solar_gm(S, ri));
-		kp3 = dt * dphi_dt(p, ri);
+		stage_rates(m, p, ri, solar_gm(S, ri), a, b, true);
+		kv3 = dt * a;
+		kp3 = dt * b;
 		ri = p.radius + 439.0 / 216.0 * kr0 - 8.0 * kr1 + 3680.0 / 513.0 * kr2 - 845.0 / 4104.0 * kr3;
 		kr4 = dt * (p.v_radial + 439.0 / 216.0 * kv0 - 8.0 * kv1 + 3680.0 / 513.0 * kv2 - 845.0 / 4104.0 * kv3);
-		kv4 = dt * dv_dt(J, ri, solar_gm(S, ri));
-		kp4 = dt * dphi_dt(p, ri);
+		stage_rates(m, p, ri, solar_gm(S, ri), a, b, true);
+		kv4 = dt * a;
+		kp4 = dt * b;
 		ri = p.radius - 8.0 / 27.0 * kr0 + 2.0 * kr1 - 3544.0 / 2565.0 * kr2 + 1859.0 / 4104.0 * kr3 - 11.0 / 40.0 * kr4;
 		kr5 = dt * (p.v_radial - 8.0 / 27.0 * kv0 + 2.0 * kv1 - 3544.0 / 2565.0 * kv2 + 1859.0 / 4104.0 * kv3 - 11.0 / 40.0 * kv4);
-		kv5 = dt * dv_dt(J, ri, solar_gm(S, ri));
-		kp5 = dt * dphi_dt(p, ri);
+		stage_rates(m, p, ri, solar_gm(S, ri), a, b, true);
+		kv5 = dt * a;
+		kp5 = dt * b;
 		const double r4 = p.radius + 25.0 / 216.0 * kr0 + 1408.0 / 2565.0 * kr2 + 2197.0 / 4104.0 * kr3 - 1.0 / 5.0 * kr4;
 		const double v4 = p.v_radial + 25.0 / 216.0 * kv0 + 1408.0 / 2565.0 * kv2 + 2197.0 / 4104.0 * kv3 - 1.0 / 5.0 * kv4;
 		const double p4 = p.phi + 25.0 / 216.0 * kp0 + 1408.0 / 2565.0 * kp2 + 2197.0 / 4104.0 * kp3 - 1.0 / 5.0 * kp4;
@@ -672,7 +776,7 @@ __device__ __forceinline__ int rk45_attempt_unrolled(const DevSolar& S, Prop& p,
 		const double v5 = p.v_radial + 16.0 / 135.0 * kv0 + 6656.0 / 12825.0 * kv2 + 28561.0 / 56430.0 * kv3 - 9.0 / 50.0 * kv4 + 2.0 / 55.0 * kv5;
 		const double p5 = p.phi + 16.0 / 135.0 * kp0 + 6656.0 / 12825.0 * kp2 + 28561.0 / 56430.0 * kp3 - 9.0 / 50.0 * kp4 + 2.0 / 55.0 * kp5;
 		const double e0 = fabs(r5 - r4), e1 = fabs(v5 - v4), e2 = fabs(p5 - p4);
-		const double new_step = next_step_size(dt, e0, e1, e2);
+		const double new_step = next_step_size_t(m, dt, e0, e1, e2);
 		const bool within = isfinite(e0) && e0 <= DMS_RK45_TOL_R_KM && isfinite(e1) && e1 <= DMS_RK45_TOL_V_KMS && isfinite(e2) && e2 <= DMS_RK45_TOL_PHI;
 		if(within)
 		{
@@ -699,6 +803,176 @@ __device__ __forceinline__ int rk45_attempt_unrolled(const DevSolar& S, Prop& p,
 		p.time_step = new_step;
 		return RK_RETRY;
 	}
+}
+
+__device__ __forceinline__ int rk45_attempt_unrolled(const DevSolar& S, Prop& p, int inner)
+{
+	IeeeMath m;
+	return rk45_attempt_t(S, p, inner, m);
+}
+
+// The IEEE attempt, out of line: the fallback of rk45_attempt_certified.
+static __device__ __noinline__ int rk45_attempt_ieee(const DevSolar& S, Prop& p, int inner)
+{
+	IeeeMath m;
+	return rk45_attempt_t(S, p, inner, m);
+}
+
+// Solar_Model::Mass as G*M for tables whose buckets hold at most one knot
+// (S.bucket_single_step): both candidate intervals are loaded with the bucket's base and the
+// interval of the search in knot_index is selected, so the lookup has no branch.  Same value
+// as solar_gm.
+__device__ __forceinline__ double solar_gm_select(const DevSolar& S, double r)
+{
+	const double x = r < 0.0 ? 0.0 : r;
+	const double xc = !(x >= 0.0) ? 0.0 : (x > DMS_RSUN_KM ? DMS_RSUN_KM : x);
+	int b = static_cast<int>(xc * S.bucket_scale);
+	b = b > S.nbuckets ? S.nbuckets : b;
+	int i = __ldg(S.bucket + b);
+	DMS_CHECK_INDEX(i, 0, S.n - 1, BOUNDS_KNOT);
+	const double r0 = __ldg(S.r + i), r1 = __ldg(S.r + i + 1);
+	const double y0 = __ldg(S.gm + i), y1 = __ldg(S.gm + i + 1);
+	const double s0 = __ldg(S.gm_s + i), s1 = __ldg(S.gm_s + i + 1);
+	const bool up = (i < S.n - 2) & (r1 <= x);
+	const double v = up ? y1 + (x - r1) * s1 : y0 + (x - r0) * s0;
+	return !isfinite(r) ? NAN : (r > DMS_RSUN_KM ? DMS_GMSUN_KM3S2 : v);
+}
+
+// One stage's dv/dt = J*J/r/r/r - gm/r/r (r clamped to >= 1 km) and, when wanted,
+// dphi/dt = J/r/r (0 in radial mode, for J = 0 or r <= 0), with the certified division and
+// without branches: every quotient by r shares one reciprocal.  A stage with 0 < r < 1 km (where
+// the reference divides J by the unclamped r) clears `good`, which hands the attempt to IEEE.
+template <bool WANT_PHI>
+__device__ __forceinline__ void cert_stage(const DevSolar& S, const Prop& p, double r, double& dv, double& dphi, bool& good)
+{
+	const double gm = solar_gm_select(S, r);
+	const double rc = r < 1.0 ? 1.0 : r;
+	const fast::Recip R = fast::recip(rc);
+	const double jj = p.J * p.J;
+	dv = fast::div(fast::div(fast::div(jj, R, good), R, good), R, good) - fast::div(fast::div(gm, R, good), R, good);
+	dphi = 0.0;
+	if(WANT_PHI)
+	{
+		const bool zero = (p.radial_mode != 0) | (p.J == 0.0) | (r <= 0.0);
+		const double q = fast::div(fast::div(p.J, R, good), R, good);
+		dphi = zero ? 0.0 : q;
+		good &= zero | (r >= 1.0);
+	}
+}
+
+// The factor of RK45_Next_Step_Size for one error component without branches: 0.84 (tol/e)^(1/4)
+// when e > 0 and the result is finite, else +inf (no limit); e outside (0, inf) divides 1.
+__device__ __forceinline__ double cert_step_factor(double tol, double e, bool& good)
+{
+	const bool use = (e > 0.0) & isfinite(e);
+	const double c = 0.84 * fast::sqrt(fast::sqrt(fast::div(tol, use ? e : 1.0, good), good), good);
+	return (use & isfinite(c)) ? c : INFINITY;
+}
+
+// The written-out attempt of rk45_attempt_t with the certified division and square root and
+// no branch before its final accept / retry decision, so that the compiler can overlap the
+// stages that do not depend on one another: the radius of stage j needs the slopes of stages
+// up to j - 2 only, so stages 0 and 1, 2 and 3, 4 and 5 are independent pairs.  `good` is
+// cleared when any certificate fails; p is then unchanged and the caller repeats the attempt
+// with IEEE arithmetic.
+__device__ __forceinline__ int rk45_attempt_cert(const DevSolar& S, Prop& p, int inner, bool& good)
+{
+	const double dt = p.time_step;
+	double kr0, kr1, kr2, kr3, kr4, kr5, kv0, kv1, kv2, kv3, kv4, kv5, kp0, kp1, kp2, kp3, kp4, kp5, ri, a;
+	kr0 = dt * p.v_radial;
+	cert_stage<true>(S, p, p.radius, a, kp0, good);
+	kv0 = dt * a;
+	kp0 = dt * kp0;
+	ri = p.radius + kr0 / 4.0;
+	kr1 = dt * (p.v_radial + kv0 / 4.0);
+	cert_stage<false>(S, p, ri, a, kp1, good);
+	kv1 = dt * a;
+	ri = p.radius + 3.0 / 32.0 * kr0 + 9.0 / 32.0 * kr1;
+	kr2 = dt * (p.v_radial + 3.0 / 32.0 * kv0 + 9.0 / 32.0 * kv1);
+	cert_stage<true>(S, p, ri, a, kp2, good);
+	kv2 = dt * a;
+	kp2 = dt * kp2;
+	ri = p.radius + 1932.0 / 2197.0 * kr0 - 7200.0 / 2197.0 * kr1 + 7296.0 / 2197.0 * kr2;
+	kr3 = dt * (p.v_radial + 1932.0 / 2197.0 * kv0 - 7200.0 / 2197.0 * kv1 + 7296.0 / 2197.0 * kv2);
+	cert_stage<true>(S, p, ri, a, kp3, good);
+	kv3 = dt * a;
+	kp3 = dt * kp3;
+	ri = p.radius + 439.0 / 216.0 * kr0 - 8.0 * kr1 + 3680.0 / 513.0 * kr2 - 845.0 / 4104.0 * kr3;
+	kr4 = dt * (p.v_radial + 439.0 / 216.0 * kv0 - 8.0 * kv1 + 3680.0 / 513.0 * kv2 - 845.0 / 4104.0 * kv3);
+	cert_stage<true>(S, p, ri, a, kp4, good);
+	kv4 = dt * a;
+	kp4 = dt * kp4;
+	ri = p.radius - 8.0 / 27.0 * kr0 + 2.0 * kr1 - 3544.0 / 2565.0 * kr2 + 1859.0 / 4104.0 * kr3 - 11.0 / 40.0 * kr4;
+	kr5 = dt * (p.v_radial - 8.0 / 27.0 * kv0 + 2.0 * kv1 - 3544.0 / 2565.0 * kv2 + 1859.0 / 4104.0 * kv3 - 11.0 / 40.0 * kv4);
+	cert_stage<true>(S, p, ri, a, kp5, good);
+	kv5 = dt * a;
+	kp5 = dt * kp5;
+	const double r4 = p.radius + 25.0 / 216.0 * kr0 + 1408.0 / 2565.0 * kr2 + 2197.0 / 4104.0 * kr3 - 1.0 / 5.0 * kr4;
+	const double v4 = p.v_radial + 25.0 / 216.0 * kv0 + 1408.0 / 2565.0 * kv2 + 2197.0 / 4104.0 * kv3 - 1.0 / 5.0 * kv4;
+	const double p4 = p.phi + 25.0 / 216.0 * kp0 + 1408.0 / 2565.0 * kp2 + 2197.0 / 4104.0 * kp3 - 1.0 / 5.0 * kp4;
+	const double r5 = p.radius + 16.0 / 135.0 * kr0 + 6656.0 / 12825.0 * kr2 + 28561.0 / 56430.0 * kr3 - 9.0 / 50.0 * kr4 + 2.0 / 55.0 * kr5;
+	const double v5 = p.v_radial + 16.0 / 135.0 * kv0 + 6656.0 / 12825.0 * kv2 + 28561.0 / 56430.0 * kv3 - 9.0 / 50.0 * kv4 + 2.0 / 55.0 * kv5;
+	const double p5 = p.phi + 16.0 / 135.0 * kp0 + 6656.0 / 12825.0 * kp2 + 28561.0 / 56430.0 * kp3 - 9.0 / 50.0 * kp4 + 2.0 / 55.0 * kp5;
+	const double e0 = fabs(r5 - r4), e1 = fabs(v5 - v4), e2 = fabs(p5 - p4);
+	// RK45_Next_Step_Size (src/Simulation_Trajectory.cpp:477-502) as selects: the factor is
+	// limited by each component in turn, clamped to [0.1, 4], and the step sanitised; non-finite
+	// errors give 0.1 x the current step
+	double factor = DMS_RK45_MAX_STEP_FACTOR;
+	const double c0 = cert_step_factor(DMS_RK45_TOL_R_KM, e0, good);
+	factor = c0 < factor ? c0 : factor;
+	const double c1 = cert_step_factor(DMS_RK45_TOL_V_KMS, e1, good);
+	factor = c1 < factor ? c1 : factor;
+	const double c2 = cert_step_factor(DMS_RK45_TOL_PHI, e2, good);
+	factor = c2 < factor ? c2 : factor;
+	factor = factor > DMS_RK45_MAX_STEP_FACTOR ? DMS_RK45_MAX_STEP_FACTOR : factor;
+	factor = factor < DMS_RK45_MIN_STEP_FACTOR ? DMS_RK45_MIN_STEP_FACTOR : factor;
+	const double grown = factor * dt;
+	const double sane = (!isfinite(grown) | (grown <= 0.0)) ? DMS_RK45_DEFAULT_STEP_S
+	                    : (grown < DMS_RK45_ABS_MAX_STEP_S ? grown : DMS_RK45_ABS_MAX_STEP_S);
+	const bool finite_err = isfinite(e0) & isfinite(e1) & isfinite(e2);
+	const double new_step = finite_err ? sane : DMS_RK45_MIN_STEP_FACTOR * dt;
+	const bool within = finite_err & (e0 <= DMS_RK45_TOL_R_KM) & (e1 <= DMS_RK45_TOL_V_KMS) & (e2 <= DMS_RK45_TOL_PHI);
+	if(!good)
+		return RK_RETRY;
+	if(within)
+	{
+		p.time = p.time + dt;
+		p.radius = r4 < 0.0 ? 0.0 : r4;
+		p.v_radial = v4;
+		p.phi = p4;
+		p.time_step = new_step;
+		return RK_ACCEPTED;
+	}
+	if(new_step < DMS_RK45_ABS_MIN_STEP_S || inner >= DMS_RK45_MAX_INNER_RETRIES)
+	{
+		const bool ok = isfinite(r4) && isfinite(v4) && isfinite(p4);
+		p.time = p.time + DMS_RK45_ABS_MIN_STEP_S;
+		if(ok)
+		{
+			p.radius = r4 < 0.0 ? 0.0 : r4;
+			p.v_radial = v4;
+			p.phi = p4;
+		}
+		p.time_step = DMS_RK45_ABS_MIN_STEP_S;
+		return RK_FORCED;
+	}
+	p.time_step = new_step;
+	return RK_RETRY;
+}
+
+// One attempt with the certified straight-line division and square root; when any certificate
+// fails (or the tables' buckets can hold two knots), the attempt is repeated from the same
+// state with IEEE arithmetic.  Either way the result is bit-identical with rk45_attempt_unrolled.
+__device__ __forceinline__ int rk45_attempt_certified(const DevSolar& S, Prop& p, int inner)
+{
+	bool good = S.bucket_single_step != 0;
+	if(good)
+	{
+		const int rk = rk45_attempt_cert(S, p, inner, good);
+		if(good)
+			return rk;
+	}
+	return rk45_attempt_ieee(S, p, inner);
 }
 
 // Runge-Kutta-Fehlberg 4(5) coefficients of src/Simulation_Trajectory.cpp:1492-1540: stage

@@ -233,16 +233,36 @@ std::string Load_Solar_Tables(const std::string& path, SolarTables& t)
 	}
 	Slopes(t.r, t.ne, t.ne_s);
 
-	// bucket acceleration for the device knot search
+	// bucket acceleration for the device knot search.  The device maps x in [0, R_sun] to bucket
+	// b = (int)(x * scale) with scale = nbuckets / R_sun (one IEEE multiply, truncation).  The
+	// base of bucket b is the knot interval of the smallest x that the device maps to b, so every
+	// x of the bucket lies in that interval or a later one; when no bucket holds more than one
+	// knot, the interval is the base or the base + 1 and the device search is one select.
+	if(n > 65535)
+		return "solar model has too many rows";
 	t.nbuckets = 8192;
+	const double scale = static_cast<double>(t.nbuckets) / DMS_RSUN_KM;
+	std::vector<double> lowest(t.nbuckets + 2, DMS_RSUN_KM);
 	t.bucket_index.resize(t.nbuckets + 1);
 	for(int b = 0; b <= t.nbuckets; b++)
 	{
-		const double x = DMS_RSUN_KM * static_cast<double>(b) / static_cast<double>(t.nbuckets);
+		// smallest double x >= 0 with (int)(x * scale) >= b
+		double x = static_cast<double>(b) / scale;
+		while(x > 0.0 && static_cast<int>(x * scale) >= b) x = std::nextafter(x, -1.0);
+		while(static_cast<int>(x * scale) < b) x = std::nextafter(x, 2.0 * DMS_RSUN_KM);
+		lowest[b] = x;
 		t.bucket_index[b] = static_cast<uint16_t>(Knot_Search(t.r, x));
 	}
-	if(n > 65535)
-		return "solar model has too many rows";
+	t.bucket_single_step = 1;
+	for(int b = 0; b < t.nbuckets; b++)
+	{
+		// the last x of bucket b is just below lowest[b + 1]: its interval must be base or base + 1
+		const double top = std::nextafter(lowest[b + 1], -1.0);
+		if(Knot_Search(t.r, top) > t.bucket_index[b] + 1)
+			t.bucket_single_step = 0;
+	}
+	if(Knot_Search(t.r, DMS_RSUN_KM) > t.bucket_index[t.nbuckets] + 1)
+		t.bucket_single_step = 0;
 	return "";
 }
 

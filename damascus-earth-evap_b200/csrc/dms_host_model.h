@@ -28,8 +28,11 @@ struct SolarTables
 	std::vector<double> nt, nt_s;    // n_i [1/km^3], node-major n x DMS_NUM_TARGETS
 	double target_mass_gev[DMS_NUM_TARGETS];
 	// bucket acceleration of the knot search: bucket b covers [b, b+1) * rsun / nbuckets,
-	// bucket_index[b] = knot interval containing the bucket start
+	// bucket_index[b] = knot interval containing the smallest radius the device maps to b;
+	// bucket_single_step = 1 when the interval of every radius of a bucket is its base or the
+	// base + 1 (no bucket holds two knots)
 	int nbuckets = 0;
+	int bucket_single_step = 0;
 	std::vector<uint16_t> bucket_index;
 };
 

@@ -19,6 +19,17 @@ namespace
 using namespace lane;
 using StrictLane = LaneT<Prop, Event>;
 
+// The written-out attempt: with the certified straight-line division and square root
+// (DMS_CERTIFIED_MATH = 1, the default; IEEE fallback per attempt) or with IEEE arithmetic.
+__device__ __forceinline__ int rk45_attempt_written_out(const DevSolar& S, Prop& p, int inner)
+{
+#if DMS_CERTIFIED_MATH
+	return rk45_attempt_certified(S, p, inner);
+#else
+	return rk45_attempt_unrolled(S, p, inner);
+#endif
+}
+
 // commit_accepted_event, src/Simulation_Trajectory.cpp:842-874.  Returns the capture energy of
 // the committed event when it was evaluated (NaN otherwise) so that the uncaptured-bound guard
 // that follows the commit reuses the same value.
@@ -126,9 +137,9 @@ __device__ __forceinline__ int free_step(const RunParams& R, const DevPoint* __r
 	}
 	L.rk_inner++;
 #if DMS_RK_UNROLLED == 2
-	const int rk = drained ? rk45_attempt_unrolled(S, L.pr, L.rk_inner) : rk45_attempt(S, L.pr, L.rk_inner);
+	const int rk = drained ? rk45_attempt_written_out(S, L.pr, L.rk_inner) : rk45_attempt(S, L.pr, L.rk_inner);
 #elif DMS_RK_UNROLLED == 1
-	const int rk = rk45_attempt_unrolled(S, L.pr, L.rk_inner);
+	const int rk = rk45_attempt_written_out(S, L.pr, L.rk_inner);
 #else
 	const int rk = rk45_attempt(S, L.pr, L.rk_inner);
 #endif
@@ -450,7 +461,91 @@ __global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double* out, int it
 		out[0] = s;
 }
 
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x)
+{
+	x += 0x9e3779b97f4a7c15ULL;
+	x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+	x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+	return x ^ (x >> 31);
+}
+
+// A double with random significand and an exponent uniform in [lo, hi].
+__device__ __forceinline__ double random_double(uint64_t bits, int lo, int hi)
+{
+	const int e = lo + static_cast<int>((bits >> 52) % static_cast<uint64_t>(hi - lo + 1));
+	const uint64_t mant = bits & 0x000fffffffffffffULL;
+	return __longlong_as_double(static_cast<long long>((static_cast<uint64_t>(e + 1023) << 52) | mant));
+}
+
+// Self-test of the certified division and square root against IEEE `/` and sqrt on n random
+// operand pairs: out[0] quotients whose certificate held but whose bits differ from IEEE (must
+// be 0), out[1] quotients whose certificate failed, out[2] and out[3] the same for the root.
+// Operands: random exponents in the ranges of the trajectory arithmetic, arbitrary bit patterns
+// (NaN, infinities, subnormals, zeros), quotients within a few ulp of representable values,
+// and exact quotients (a power-of-two divisor).  Division and square root never land exactly
+// halfway between two doubles, so round-to-nearest has no ties to test.
+__global__ void certified_math_check_kernel(uint64_t n, uint64_t seed, unsigned long long* out)
+{
+	unsigned long long c[4] = {0, 0, 0, 0};
+	for(uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < n; k += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+	{
+		const uint64_t h1 = splitmix64(seed ^ (k * 0x2545f4914f6cdd1dULL)), h2 = splitmix64(h1), h3 = splitmix64(h2);
+		double a, b;
+		switch(k & 3)
+		{
+			case 0:  // the trajectory ranges: km, km/s, s, km^3/s^2
+				a = random_double(h1, -40, 70);
+				b = random_double(h2, -20, 40);
+				break;
+			case 1:  // any bit pattern
+				a = __longlong_as_double(static_cast<long long>(h1));
+				b = __longlong_as_double(static_cast<long long>(h2));
+				break;
+			case 2:
+			{  // dividend a few ulp away from b * q for a random q
+				b = random_double(h1, -30, 30);
+				const double q = random_double(h2, -30, 30);
+				const long long d = static_cast<long long>(h3 % 7) - 3;
+				a = __longlong_as_double(__double_as_longlong(__dmul_rn(b, q)) + d);
+				break;
+			}
+			default:
+			{  // exact quotients: a power-of-two divisor
+				const double m = random_double(h1, -10, 10);
+				b = ldexp(1.0, static_cast<int>(h2 % 41) - 20);
+				a = __dmul_rn(b, m);
+				break;
+			}
+		}
+		if(h3 & 1)
+			a = -a;
+		bool ok = true;
+		const double q = fast::div(a, b, ok);
+		const double ref = a / b;
+		if(!ok)
+			c[1]++;
+		else if(__double_as_longlong(q) != __double_as_longlong(ref) && !(isnan(q) && isnan(ref)))
+			c[0]++;
+		const double x = fabs(a);
+		bool ok2 = true;
+		const double sq = fast::sqrt(x, ok2);
+		const double sref = sqrt(x);
+		if(!ok2)
+			c[3]++;
+		else if(__double_as_longlong(sq) != __double_as_longlong(sref) && !(isnan(sq) && isnan(sref)))
+			c[2]++;
+	}
+	for(int i = 0; i < 4; i++)
+		if(c[i])
+			atomicAdd(out + i, c[i]);
+}
+
 }	// namespace
+
+void Check_Certified_Math(uint64_t n, uint64_t seed, unsigned long long* out, int sm_count, cudaStream_t stream)
+{
+	certified_math_check_kernel<<<sm_count * 8, 256, 0, stream>>>(n, seed, out);
+}
 
 double Measure_FP64_Peak(int sm_count, cudaStream_t stream)
 {

@@ -20,6 +20,11 @@
 #ifndef DMS_RK_UNROLLED
 #define DMS_RK_UNROLLED 1
 #endif
+// FP64 RK45 attempts with the certified straight-line division and square root of
+// dms_fastmath.cuh (1) or with IEEE `/` and sqrt (0); the results are the same bits.
+#ifndef DMS_CERTIFIED_MATH
+#define DMS_CERTIFIED_MATH 1
+#endif
 #ifndef DMS_RK_UNROLLED_MIXED
 #define DMS_RK_UNROLLED_MIXED 1
 #endif
@@ -136,5 +141,8 @@ int Trajectory_Mixed_Max_Blocks_Per_SM(int threads);
 int Trajectory_Kernel_Registers();
 int Trajectory_Max_Blocks_Per_SM(int threads);
 double Measure_FP64_Peak(int sm_count, cudaStream_t stream);
+// Self-test of the certified division and square root (dms_fastmath.cuh) against IEEE on n
+// random operand pairs; out (4 device counters, zeroed by the caller) as in dms_check_certified_math.
+void Check_Certified_Math(uint64_t n, uint64_t seed, unsigned long long* out, int sm_count, cudaStream_t stream);
 
 }	// namespace dms

@@ -169,6 +169,7 @@ def library():
     lib.dms_num_bins.restype = c.c_int
     lib.dms_last_kernel_ms.argtypes = [vp, c.POINTER(c.c_double)]
     lib.dms_measure_fp64_peak.argtypes = [vp, c.POINTER(c.c_double)]
+    lib.dms_check_certified_math.argtypes = [vp, c.c_uint64, c.c_uint64, c.POINTER(c.c_uint64)]
     lib.dms_get_reflection_spectrum.argtypes = [vp, c.c_int, c.c_uint32, c.c_uint32, c.c_double, c.POINTER(ReflectionSpectrum)]
     lib.dms_reflection_spectrum_pdf.argtypes = [vp, c.c_int, c.c_uint32, c.c_uint32, vp, c.c_size_t, vp]
     lib.dms_set_progress_callback.argtypes = [vp, PROGRESS_FN, vp, c.c_double]
@@ -394,6 +395,12 @@ class Engine:
         t = ctypes.c_double(0.0)
         self._check(self.lib.dms_measure_fp64_peak(self.h, ctypes.byref(t)))
         return t.value
+
+    def check_certified_math(self, n, seed=1):
+        """dms_check_certified_math: (div mismatches, div fallbacks, sqrt mismatches, sqrt fallbacks)."""
+        counts = (ctypes.c_uint64 * 4)()
+        self._check(self.lib.dms_check_certified_math(self.h, n, seed, counts))
+        return tuple(int(x) for x in counts)
 
     def reset_results(self, point):
         self._check(self.lib.dms_reset_results(self.h, point))

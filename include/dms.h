@@ -364,6 +364,13 @@ int dms_last_kernel_ms(const dms_ctx* ctx, double* ms);
  * kernel (a diagnostic with no reference counterpart). */
 int dms_measure_fp64_peak(dms_ctx* ctx, double* tflops);
 
+/* Self-test of the certified straight-line FP64 division and square root that the FP64 RK45
+ * attempts use (a diagnostic with no reference counterpart): n random operand pairs, each
+ * divided and square-rooted both ways.  counts[0] = quotients whose certificate held but whose
+ * bits differ from IEEE a / b (must be 0), counts[1] = quotients whose certificate failed (the
+ * kernel then falls back to IEEE), counts[2], counts[3] the same for sqrt. */
+int dms_check_certified_math(dms_ctx* ctx, uint64_t n, uint64_t seed, uint64_t* counts);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,8 +48,8 @@ def _init(kind, params, grid):
 
 
 def _work(task):
-    seed, first, count, capture_mode, max_scatterings = task
-    res = _IMPL.run_records(seed, 0, first, count, capture_mode=capture_mode, max_scatterings=max_scatterings,
+    seed, point, first, count, capture_mode, max_scatterings = task
+    res = _IMPL.run_records(seed, point, first, count, capture_mode=capture_mode, max_scatterings=max_scatterings,
                             histograms=not capture_mode)
     recs = res["records"]
     out = np.zeros(count, dtype=OUTCOME_DTYPE)
@@ -73,13 +73,15 @@ def _work(task):
 
 
 def run_ensemble(kind, params, seed, first, count, capture_mode=False, max_scatterings=10 ** 6, grid=None,
-                 workers=None, chunk=128):
+                 workers=None, chunk=128, point=0):
     """Runs ids [first, first + count) of one point through `kind` ("reference" or "oracle") on
     `workers` processes (default: every host core) and returns the aggregate (counters,
     histograms, events) with the per-trajectory `outcomes` sorted by id.  `grid` (oracle only)
-    replaces the oracle's own rate grid."""
+    replaces the oracle's own rate grid.  `point` is the point index of the draw streams, which
+    are keyed by (seed, point): it must be the engine's point id for a trajectory-by-trajectory
+    comparison."""
     workers = workers or os.cpu_count() or 1
-    tasks = [(seed, s, min(chunk, first + count - s), capture_mode, max_scatterings)
+    tasks = [(seed, point, s, min(chunk, first + count - s), capture_mode, max_scatterings)
              for s in range(first, first + count, chunk)]
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers, initializer=_init, initargs=(kind, params, grid)) as pool:

@@ -56,7 +56,7 @@ def test_replay_on_the_device_built_grid(engine, name):
     opts = dms_b200.run_opts(seed=cfg["seed"], capture_mode=cfg["capture_mode"], max_scatterings=cfg["max_scatterings"],
                              time_limit_s=300.0)
     mine = engine.run_records(pid, 0, n, opts)["records"]
-    kw = dict(capture_mode=cfg["capture_mode"], max_scatterings=cfg["max_scatterings"])
+    kw = dict(capture_mode=cfg["capture_mode"], max_scatterings=cfg["max_scatterings"], point=pid)
     on_device_grid = cpu_pool.run_ensemble("oracle", p, cfg["seed"], 0, n, grid=grid, **kw)["outcomes"]
     on_own_grid = cpu_pool.run_ensemble("oracle", p, cfg["seed"], 0, n, **kw)["outcomes"]
 

@@ -77,7 +77,7 @@ def test_engine_ensemble_agrees_with_the_reference_run(engine, name):
     mine = engine.results(pid, events_capacity=1 << 17)
     mine_out = outcome_table(engine.run_records(pid, 0, n, opts)["records"], n)
     ref = cpu_pool.run_ensemble("reference", p, cfg["seed"], 0, n, capture_mode=cfg["capture_mode"],
-                                max_scatterings=cfg["max_scatterings"])
+                                max_scatterings=cfg["max_scatterings"], point=pid)
     ro = ref["outcomes"]
     same = ((mine_out["nscat"] == ro["nscat"]) & (mine_out["reason"] == ro["reason"]) &
             (mine_out["flags"] == ro["flags"]) & (mine_out["draws"] == ro["draws"]))
