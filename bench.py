@@ -259,6 +259,14 @@ def run_engine_arm(args):
                                     precision=prec) for prec in (fp64, mixed)}
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     peak = engine.fp64_peak_tflops()
+    # the autotuner picks block size, blocks per SM, queue chunk and the warp batching of each
+    # form on this point (short trial launches over fresh ids; results never depend on them)
+    tuning = {}
+    if args.autotune_seconds > 0:
+        for prec in (fp64, mixed):
+            tuned, trials = engine.autotune([(pids[0], 0, TRAJECTORIES)], opts[prec], trial_seconds=args.autotune_seconds)
+            opts[prec] = tuned
+            tuning["fp64" if prec == fp64 else "mixed"] = dict(dms_b200.lane_options(tuned), trials=trials)
 
     def barrier():
         torch.cuda.synchronize()
@@ -444,6 +452,9 @@ def run_engine_arm(args):
                 "clocks": mix_clocks,
                 "gpu_launches": 2,
             }
+        if tuning:
+            line["autotune"] = dict(tuning, note="0 = the library default; trials of %.2f s over fresh ids, scored by "
+                                                 "accepted steps per second" % args.autotune_seconds)
         if grid is not None:
             line["grid_20_points"] = grid
         if stress is not None:
@@ -622,6 +633,8 @@ def main():
     ap.add_argument("--steady-seconds", type=float, default=2.0,
                     help="length of the steady-state measurement per form (0 skips it)")
     ap.add_argument("--repeats", type=int, default=3, help="runs of the timed launch and of the e2e leg (median reported)")
+    ap.add_argument("--autotune-seconds", type=float, default=0.2,
+                    help="trial length of the launch autotuner run before the timed launches (0 skips it)")
     ap.add_argument("--grid-seconds", type=float, default=20.0,
                     help="bounded 20-point grid launch per form inside the bench line (0 skips it)")
     ap.add_argument("--stress-seconds", type=float, default=10.0,

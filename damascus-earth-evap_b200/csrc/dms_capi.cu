@@ -201,7 +201,21 @@ int Check_Run_Opts(dms_ctx* ctx, const dms_run_opts* o)
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "unsupported precision");
 	if(o->threads_per_block != 0 && (o->threads_per_block % 32 != 0 || o->threads_per_block > 128))
 		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "threads_per_block must be a multiple of 32 up to 128");
+	if(o->queue_chunk > 1024)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "queue_chunk must be at most 1024");
+	if(o->scatter_batch > 32 || o->final_batch > 32 || o->scatter_wait > 1024 || o->final_wait > 1024)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "warp batching: batches up to 32 lanes, waits up to 1024 iterations");
 	return DMS_OK;
+}
+
+// The lane-scheduling options of a launch (dms_run_opts, 0 = default).
+void Apply_Lane_Options(RunParams& p, const dms_run_opts* o)
+{
+	p.queue_chunk = o->queue_chunk ? o->queue_chunk : 1u;
+	p.scatter_batch = o->scatter_batch ? static_cast<int>(o->scatter_batch) : 16;
+	p.scatter_wait = o->scatter_wait ? static_cast<int>(o->scatter_wait) : 32;
+	p.final_batch = o->final_batch ? static_cast<int>(o->final_batch) : 8;
+	p.final_wait = o->final_wait ? static_cast<int>(o->final_wait) : 32;
 }
 
 // One persistent launch over the given work; polls for completion, enforcing the wall-clock
@@ -213,6 +227,7 @@ int Launch_And_Wait(dms_ctx* ctx, const dms_run_opts* o, RunParams& p)
 	p.wall_limit_ns = static_cast<uint64_t>(o->max_trajectory_wall_time_s * 1.0e9);
 	if(o->max_trajectory_wall_time_s > 0.0 && p.wall_limit_ns == 0)
 		p.wall_limit_ns = 1;
+	Apply_Lane_Options(p, o);
 	const int threads = o->threads_per_block ? static_cast<int>(o->threads_per_block) : 128;
 	const bool mixed = o->precision == DMS_PRECISION_MIXED;
 	const int max_per_sm = mixed ? Trajectory_Mixed_Max_Blocks_Per_SM(threads) : Trajectory_Max_Blocks_Per_SM(threads);
@@ -799,6 +814,185 @@ int dms_run(dms_ctx* ctx, const dms_run_opts* opts, const dms_work_range* ranges
 	return rc;
 }
 
+// ---- autotuner ------------------------------------------------------------------------------
+namespace
+{
+// One trial of the autotuner: a launch stopped after `seconds` over fresh ids (from 2^40) of the
+// given points, its results in the scratch accumulators `scratch`; returns accepted free steps
+// per second (finished and unfinished trajectories), or a negative value on failure.
+struct TuneScratch
+{
+	unsigned long long* counters = nullptr;
+	double* hists = nullptr;
+	dms_evaporation_event* events = nullptr;
+	unsigned long long* event_count = nullptr;
+	dms_reflection* refl = nullptr;
+	unsigned long long* refl_count = nullptr;
+	uint64_t capacity = 256;
+	void Free()
+	{
+		cudaFree(counters);
+		cudaFree(hists);
+		cudaFree(events);
+		cudaFree(event_count);
+		cudaFree(refl);
+		cudaFree(refl_count);
+	}
+};
+
+double Tune_Trial(dms_ctx* ctx, const dms_run_opts& o, const std::vector<int32_t>& pts, uint64_t per_point, uint64_t first,
+                  const TuneScratch& t, void* d_ranges)
+{
+	const int n = static_cast<int>(pts.size());
+	const size_t np = ctx->points.size();
+	if(cudaMemsetAsync(t.counters, 0, sizeof(unsigned long long) * DMS_NUM_COUNTERS * np, ctx->stream) != cudaSuccess ||
+	   cudaMemsetAsync(t.event_count, 0, sizeof(unsigned long long) * np, ctx->stream) != cudaSuccess ||
+	   cudaMemsetAsync(t.refl_count, 0, sizeof(unsigned long long) * np, ctx->stream) != cudaSuccess)
+		return -1.0;
+	std::vector<uint64_t> firsts(n, first), offsets(n + 1);
+	for(int k = 0; k <= n; k++) offsets[k] = per_point * static_cast<uint64_t>(k);
+	char* dc = static_cast<char*>(d_ranges);
+	const size_t off_offset = sizeof(uint64_t) * n, off_point = sizeof(uint64_t) * (2 * n + 1);
+	std::vector<char> buf(off_point + sizeof(int32_t) * n);
+	std::memcpy(buf.data(), firsts.data(), sizeof(uint64_t) * n);
+	std::memcpy(buf.data() + off_offset, offsets.data(), sizeof(uint64_t) * (n + 1));
+	std::memcpy(buf.data() + off_point, pts.data(), sizeof(int32_t) * n);
+	if(cudaMemcpy(d_ranges, buf.data(), buf.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+		return -1.0;
+	RunParams p{};
+	p.range_first = reinterpret_cast<const uint64_t*>(dc);
+	p.range_offset = reinterpret_cast<const uint64_t*>(dc + off_offset);
+	p.range_point = reinterpret_cast<const int32_t*>(dc + off_point);
+	p.n_ranges = n;
+	p.total = per_point * static_cast<uint64_t>(n);
+	p.counters = t.counters;
+	p.hists = t.hists;
+	p.events = t.events;
+	p.event_count = t.event_count;
+	p.event_capacity = t.capacity;
+	p.reflections = t.refl;
+	p.reflection_count = t.refl_count;
+	const int rc = Launch_And_Wait(ctx, &o, p);
+	if(rc != DMS_OK && rc != DMS_ERR_CANCELLED)
+		return -1.0;
+	std::vector<unsigned long long> c(DMS_NUM_COUNTERS * np);
+	if(cudaMemcpy(c.data(), t.counters, sizeof(unsigned long long) * c.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+		return -1.0;
+	double steps = 0.0;
+	for(int32_t pt : pts)
+	{
+		const unsigned long long* q = c.data() + static_cast<size_t>(pt) * DMS_NUM_COUNTERS;
+		steps += static_cast<double>(q[DMS_CNT_RK_STEPS] + q[DMS_CNT_UNFINISHED_RK_STEPS]);
+	}
+	return ctx->last_kernel_ms > 0.0 ? steps / (ctx->last_kernel_ms * 1.0e-3) : -1.0;
+}
+}	// namespace
+
+int dms_autotune(dms_ctx* ctx, const dms_run_opts* base, const dms_work_range* ranges, int n_ranges, double trial_seconds,
+                 dms_run_opts* tuned, int* trials)
+{
+	if(!ctx)
+		return DMS_ERR_INVALID_ARGUMENT;
+	DMS_NOT_IN_FLIGHT(ctx);
+	int rc = Check_Run_Opts(ctx, base);
+	if(rc != DMS_OK)
+		return rc;
+	if(!tuned || n_ranges <= 0 || !ranges || !(trial_seconds > 0.0) || trial_seconds > 60.0)
+		return Fail(ctx, DMS_ERR_INVALID_ARGUMENT, "autotune: ranges, an output and a trial time in (0, 60] s are required");
+	std::vector<int32_t> pts;
+	for(int k = 0; k < n_ranges; k++)
+	{
+		if(ranges[k].point_id < 0 || ranges[k].point_id >= static_cast<int>(ctx->points.size()))
+			return Fail(ctx, DMS_ERR_NO_POINT, "work range names an unknown point");
+		if(std::find(pts.begin(), pts.end(), ranges[k].point_id) == pts.end())
+			pts.push_back(ranges[k].point_id);
+	}
+	DMS_CUDA(ctx, cudaSetDevice(ctx->device));
+	const size_t np = ctx->points.size();
+	TuneScratch t;
+	struct Guard
+	{
+		TuneScratch& t;
+		void* ranges = nullptr;
+		~Guard()
+		{
+			t.Free();
+			cudaFree(ranges);
+		}
+	} guard{t};
+	DMS_CUDA(ctx, cudaMalloc(&t.counters, sizeof(unsigned long long) * DMS_NUM_COUNTERS * np));
+	DMS_CUDA(ctx, cudaMalloc(&t.hists, sizeof(double) * DMS_NUM_HISTS * DMS_NUM_BINS * np));
+	DMS_CUDA(ctx, cudaMalloc(&t.events, sizeof(dms_evaporation_event) * t.capacity * np));
+	DMS_CUDA(ctx, cudaMalloc(&t.event_count, sizeof(unsigned long long) * np));
+	DMS_CUDA(ctx, cudaMalloc(&t.refl, sizeof(dms_reflection) * t.capacity * np));
+	DMS_CUDA(ctx, cudaMalloc(&t.refl_count, sizeof(unsigned long long) * np));
+	DMS_CUDA(ctx, cudaMalloc(&guard.ranges, (sizeof(uint64_t) * 2 + sizeof(int32_t)) * (pts.size() + 1)));
+	// enough ids that no trial drains its queue: a million per point, fresh for every trial
+	const uint64_t per_point = 1ULL << 20;
+	dms_run_opts best = *base;
+	best.time_limit_s = trial_seconds;
+	best.iteration_budget = 0;
+	int n_trials = 0;
+	uint64_t next_first = 1ULL << 40;
+	auto score = [&](const dms_run_opts& o) {
+		n_trials++;
+		const double v = Tune_Trial(ctx, o, pts, per_point, next_first, t, guard.ranges);
+		next_first += per_point;
+		return v;
+	};
+	double best_score = score(best);
+	if(!(best_score > 0.0))
+		return Fail(ctx, DMS_ERR_CUDA, "autotune: the first trial launch failed");
+	struct Knob
+	{
+		uint32_t dms_run_opts::*field;
+		std::vector<uint32_t> values;
+	};
+	const std::vector<Knob> knobs = {
+		{&dms_run_opts::threads_per_block, {64, 96, 128}},
+		{&dms_run_opts::blocks_per_sm, {2, 3, 4}},
+		{&dms_run_opts::queue_chunk, {1, 2, 4}},
+		{&dms_run_opts::scatter_batch, {8, 16, 24, 32}},
+		{&dms_run_opts::scatter_wait, {16, 32, 64, 128}},
+		{&dms_run_opts::final_batch, {4, 8, 16}},
+		{&dms_run_opts::final_wait, {16, 32, 64}},
+	};
+	// coordinate descent: a value replaces the current one only when it is at least 2 % faster
+	// (the run-to-run spread of a short trial)
+	for(int pass = 0; pass < 2; pass++)
+	{
+		bool changed = false;
+		for(const Knob& k : knobs)
+			for(uint32_t v : k.values)
+			{
+				if(best.*(k.field) == v)
+					continue;
+				dms_run_opts trial = best;
+				trial.*(k.field) = v;
+				const double sc = score(trial);
+				if(sc > 1.02 * best_score)
+				{
+					best = trial;
+					best_score = sc;
+					changed = true;
+				}
+			}
+		if(!changed)
+			break;
+	}
+	*tuned = *base;
+	tuned->threads_per_block = best.threads_per_block;
+	tuned->blocks_per_sm = best.blocks_per_sm;
+	tuned->queue_chunk = best.queue_chunk;
+	tuned->scatter_batch = best.scatter_batch;
+	tuned->scatter_wait = best.scatter_wait;
+	tuned->final_batch = best.final_batch;
+	tuned->final_wait = best.final_wait;
+	if(trials)
+		*trials = n_trials;
+	return DMS_OK;
+}
+
 int dms_run_records(dms_ctx* ctx, const dms_run_opts* opts, int point_id, uint64_t first, uint64_t count, dms_traj_record* records,
                     double* hist_dt, double* hist_v2dt)
 {
@@ -1113,6 +1307,7 @@ int dms_run_records_noalloc(dms_ctx* ctx, const dms_run_opts* opts, int point_id
 	if(opts->max_trajectory_wall_time_s > 0.0 && p.wall_limit_ns == 0)
 		p.wall_limit_ns = 1;
 	p.ic_max_attempts = 1 << 20;
+	Apply_Lane_Options(p, opts);
 	p.counters = ctx->d_counters;
 	p.hists = ctx->d_hists;
 	p.events = ctx->d_events;

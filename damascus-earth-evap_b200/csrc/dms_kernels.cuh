@@ -86,6 +86,10 @@ struct RunParams
 	double boundary;          // km
 	uint64_t iteration_budget;
 	uint64_t wall_limit_ns;  // per-trajectory wall-clock limit (max_trajectory_wall_time_sec); 0 = none
+	// lane scheduling (dms_run_opts; never changes results): ids claimed per queue fetch and
+	// the warp batching of scatterings and terminations
+	uint32_t queue_chunk;
+	int scatter_batch, scatter_wait, final_batch, final_wait;
 	int ic_max_attempts;
 	// accumulators (accumulate mode)
 	unsigned long long* counters;   // n_points x DMS_NUM_COUNTERS

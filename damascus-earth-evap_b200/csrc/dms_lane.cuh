@@ -665,18 +665,6 @@ __device__ __forceinline__ int finish_scatter(const RunParams& R, const DevPoint
 	return PH_SEGMENT;
 }
 
-#ifndef DMS_SCATTER_BATCH
-#define DMS_SCATTER_BATCH 16
-#endif
-#ifndef DMS_SCATTER_MAX_WAIT
-#define DMS_SCATTER_MAX_WAIT 32
-#endif
-#ifndef DMS_FINAL_BATCH
-#define DMS_FINAL_BATCH 8
-#endif
-#ifndef DMS_FINAL_MAX_WAIT
-#define DMS_FINAL_MAX_WAIT 32
-#endif
 
 template <class Lane, class Step>
 __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
@@ -700,6 +688,8 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	int phase = PH_FETCH;
 	int scatter_wait = 0;
 	int final_wait = 0;
+	// the lane's claimed ids [q_next, q_end): R.queue_chunk ids per claim
+	uint64_t q_next = 0, q_end = 0;
 	const unsigned int lane_bit = 1u << (threadIdx.x & 31);
 	// Every lane stays in the loop until its whole warp is done (a lane without work waits in
 	// PH_DONE), and leaves only together with the others.  So the warp's collective steps
@@ -733,15 +723,26 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 		}
 		if(phase == PH_FETCH)
 		{
-			// warp-aggregated claim of one work index per lane that needs one
+			// warp-aggregated claim of R.queue_chunk work indices per lane whose claimed ids
+			// are used up
 			const unsigned int mask = __activemask();
-			const int leader = __ffs(mask) - 1;
-			const unsigned int rank = __popc(mask & (lane_bit - 1u));
-			unsigned long long base = 0;
-			if((threadIdx.x & 31) == leader)
-				base = atomicAdd(R.queue_head, static_cast<unsigned long long>(__popc(mask)));
-			base = __shfl_sync(mask, base, leader);
-			const uint64_t w = base + rank;
+			const bool need = !(q_next < q_end);
+			const unsigned int need_mask = __ballot_sync(mask, need);
+			if(need_mask != 0u)
+			{
+				const int leader = __ffs(need_mask) - 1;
+				const unsigned int rank = __popc(need_mask & (lane_bit - 1u));
+				unsigned long long base = 0;
+				if((threadIdx.x & 31) == leader)
+					base = atomicAdd(R.queue_head, static_cast<unsigned long long>(__popc(need_mask)) * R.queue_chunk);
+				base = __shfl_sync(mask, base, leader);
+				if(need)
+				{
+					q_next = base + static_cast<uint64_t>(rank) * R.queue_chunk;
+					q_end = q_next + R.queue_chunk;
+				}
+			}
+			const uint64_t w = q_next++;
 			if(w >= R.total)
 			{
 				*reinterpret_cast<volatile int*>(&queue_drained) = 1;
@@ -755,7 +756,7 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 		if(phase == PH_STEP)
 			phase = step(R, P, m_dm, L, hist, *reinterpret_cast<volatile int*>(&queue_drained));
 		// Scatterings wait until several lanes of the warp have one (or one has waited
-		// DMS_SCATTER_MAX_WAIT iterations, or no lane is stepping), so that the scattering code
+		// R.scatter_wait iterations, or no lane is stepping), so that the scattering code
 		// runs for many lanes at once.  A lane's draws do not depend on when it scatters.
 		{
 			const unsigned int grp = FULL_WARP;
@@ -763,8 +764,8 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 			if(waiting != 0u)
 			{
 				const unsigned int stepping = __ballot_sync(grp, phase == PH_STEP);
-				const bool go = __popc(waiting) >= DMS_SCATTER_BATCH || stepping == 0u ||
-				                __any_sync(grp, phase == PH_SCATTER && scatter_wait >= DMS_SCATTER_MAX_WAIT);
+				const bool go = __popc(waiting) >= R.scatter_batch || stepping == 0u ||
+				                __any_sync(grp, phase == PH_SCATTER && scatter_wait >= R.scatter_wait);
 				if(go)
 				{
 					int target = TARGET_FAILED;
@@ -786,8 +787,8 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 			if(ending != 0u)
 			{
 				const unsigned int stepping = __ballot_sync(grp, phase == PH_STEP);
-				const bool go = __popc(ending) >= DMS_FINAL_BATCH || stepping == 0u ||
-				                __any_sync(grp, phase == PH_FINAL && final_wait >= DMS_FINAL_MAX_WAIT);
+				const bool go = __popc(ending) >= R.final_batch || stepping == 0u ||
+				                __any_sync(grp, phase == PH_FINAL && final_wait >= R.final_wait);
 				if(go)
 				{
 					if(phase == PH_FINAL)

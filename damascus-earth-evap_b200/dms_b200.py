@@ -60,7 +60,11 @@ class RunOpts(ctypes.Structure):
                 ("precision", ctypes.c_int32), ("threads_per_block", ctypes.c_uint32),
                 ("blocks_per_sm", ctypes.c_uint32), ("queue_chunk", ctypes.c_uint32),
                 ("iteration_budget", ctypes.c_uint64), ("time_limit_s", ctypes.c_double),
-                ("max_trajectory_wall_time_s", ctypes.c_double)]
+                ("max_trajectory_wall_time_s", ctypes.c_double), ("scatter_batch", ctypes.c_uint32),
+                ("scatter_wait", ctypes.c_uint32), ("final_batch", ctypes.c_uint32), ("final_wait", ctypes.c_uint32)]
+
+LANE_OPTION_NAMES = ("threads_per_block", "blocks_per_sm", "queue_chunk", "scatter_batch", "scatter_wait", "final_batch",
+                     "final_wait")
 
 
 class WorkRange(ctypes.Structure):
@@ -162,6 +166,8 @@ def library():
     lib.dms_default_run_opts.argtypes = [c.POINTER(RunOpts)]
     lib.dms_default_run_opts.restype = None
     lib.dms_run.argtypes = [vp, c.POINTER(RunOpts), c.POINTER(WorkRange), c.c_int]
+    lib.dms_autotune.argtypes = [vp, c.POINTER(RunOpts), c.POINTER(WorkRange), c.c_int, c.c_double, c.POINTER(RunOpts),
+                                 c.POINTER(c.c_int)]
     lib.dms_run_records.argtypes = [vp, c.POINTER(RunOpts), c.c_int, c.c_uint64, c.c_uint64, c.POINTER(TrajRecord), vp, vp]
     lib.dms_run_records_noalloc.argtypes = [vp, c.POINTER(RunOpts), c.c_int, c.c_uint64, c.c_uint64, vp, vp, vp]
     lib.dms_get_results.argtypes = [vp, c.c_int, c.POINTER(PointResults)]
@@ -189,7 +195,7 @@ PRECISION_MIXED = 1
 
 def run_opts(seed=1, capture_mode=False, max_scatterings=10 ** 14, max_free_steps=10 ** 12, boundary_rsun=2.0,
              threads_per_block=0, blocks_per_sm=0, time_limit_s=0.0, iteration_budget=0, precision=PRECISION_FP64,
-             max_trajectory_wall_time_s=0.0):
+             max_trajectory_wall_time_s=0.0, queue_chunk=0, scatter_batch=0, scatter_wait=0, final_batch=0, final_wait=0):
     o = RunOpts()
     library().dms_default_run_opts(ctypes.byref(o))
     o.seed = seed
@@ -203,7 +209,14 @@ def run_opts(seed=1, capture_mode=False, max_scatterings=10 ** 14, max_free_step
     o.iteration_budget = iteration_budget
     o.precision = precision
     o.max_trajectory_wall_time_s = max_trajectory_wall_time_s
+    o.queue_chunk = queue_chunk
+    o.scatter_batch, o.scatter_wait, o.final_batch, o.final_wait = scatter_batch, scatter_wait, final_batch, final_wait
     return o
+
+
+def lane_options(opts):
+    """The lane-scheduling fields of a RunOpts (the autotuner's knobs) as a dict."""
+    return {k: int(getattr(opts, k)) for k in LANE_OPTION_NAMES}
 
 
 class EngineError(RuntimeError):
@@ -276,6 +289,16 @@ class Engine:
         ranges = list(ranges)
         arr = (WorkRange * len(ranges))(*[WorkRange(p, 0, f, c) for p, f, c in ranges])
         self._check(self.lib.dms_run(self.h, ctypes.byref(opts), arr, len(ranges)))
+
+    def autotune(self, ranges, opts, trial_seconds=0.25):
+        """dms_autotune: returns (tuned RunOpts, number of trial launches)."""
+        ranges = list(ranges)
+        arr = (WorkRange * len(ranges))(*[WorkRange(p, 0, f, c) for p, f, c in ranges])
+        tuned = RunOpts()
+        n = ctypes.c_int(0)
+        self._check(self.lib.dms_autotune(self.h, ctypes.byref(opts), arr, len(ranges), trial_seconds, ctypes.byref(tuned),
+                                          ctypes.byref(n)))
+        return tuned, n.value
 
     def run_records(self, point, first, count, opts, histograms=False):
         recs = (TrajRecord * count)()

@@ -191,9 +191,10 @@ typedef struct
 	uint64_t max_free_steps;           /* maximum_free_time_steps */
 	double boundary_radius_rsun;       /* initial_and_final_radius / R_sun (2.0) */
 	int32_t precision;                 /* DMS_PRECISION_* */
-	uint32_t threads_per_block;        /* 0 = default */
-	uint32_t blocks_per_sm;            /* 0 = default */
-	uint32_t queue_chunk;              /* trajectories claimed per queue fetch; 0 = default */
+	uint32_t threads_per_block;        /* 32, 64, 96 or 128; 0 = 128 */
+	uint32_t blocks_per_sm;            /* resident blocks per SM; 0 = as many as fit */
+	uint32_t queue_chunk;              /* trajectory ids a lane claims from the work queue at a time
+	                                      (1..1024); 0 = 1 */
 	uint64_t iteration_budget;         /* per-lane loop-iteration bound; 0 = default */
 	double time_limit_s;               /* wall-clock bound of one launch, enforced through the
 	                                      cancel flag; 0 = none */
@@ -201,6 +202,16 @@ typedef struct
 	                                      on its lane exceeds it ends with
 	                                      DMS_REASON_WALL_TIME_LIMIT (checked before and after each
 	                                      RK45 step, src/Simulation_Trajectory.cpp:824-840); 0 = none */
+	/* Warp batching of the rare phases (no reference counterpart; results do not depend on it):
+	 * a lane that reaches a scattering point (a termination) waits until scatter_batch
+	 * (final_batch) lanes of its warp are there, or it has waited scatter_wait (final_wait)
+	 * loop iterations, or no lane of the warp is stepping; then the warp runs the scattering
+	 * (termination) code once for all of them.  0 = defaults 16 / 32 / 8 / 32; batches up to
+	 * 32, waits up to 1024. */
+	uint32_t scatter_batch;
+	uint32_t scatter_wait;
+	uint32_t final_batch;
+	uint32_t final_wait;
 } dms_run_opts;
 
 typedef struct
@@ -212,6 +223,18 @@ typedef struct
 } dms_work_range;
 
 void dms_default_run_opts(dms_run_opts* opts);
+
+/* Autotuner of the launch (no reference counterpart): picks threads_per_block, blocks_per_sm,
+ * queue_chunk and the warp-batching thresholds (the lane-compaction interval of the persistent
+ * kernel) for the points of `ranges` and the precision of `base`.  Each trial is a launch of
+ * trial_seconds wall time over fresh trajectory ids of those points (ids from 2^40 on, results
+ * kept in a scratch accumulator, so the points' own results are untouched), scored by accepted
+ * free steps per second; the parameters are searched one at a time from the defaults
+ * (coordinate descent, two passes).  *tuned receives `base` with the best setting; the chosen
+ * setting changes throughput only, never results (every draw is keyed by trajectory id).
+ * trials (may be NULL) receives the number of trial launches. */
+int dms_autotune(dms_ctx* ctx, const dms_run_opts* base, const dms_work_range* ranges, int n_ranges, double trial_seconds,
+                 dms_run_opts* tuned, int* trials);
 
 /* Simulates every trajectory of the given ranges in one persistent launch and adds the
  * outcomes to the per-point accumulators (counters, the four 2000-bin histograms with their

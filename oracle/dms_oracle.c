@@ -145,6 +145,13 @@ struct dms_oracle
 	/* per-trajectory scatter trace */
 	double* trace;
 	size_t trace_capacity, trace_length;
+	/* reflection-spectrum sample of the current trajectory (speed at 1 AU, cosine to the Sun's
+	 * velocity), or NULL */
+	double* reflection;
+	double* reflection_base;
+	/* when non-NULL: 7 doubles (t, x, v) per trajectory that replace the event after the initial
+	 * Kepler shift (the initial conditions still run, for their draws) */
+	const double* start_base;
 };
 
 static double next_uniform(dms_oracle* o) { return dms_draw_uniform(o->seed, o->point, o->traj, o->draw_index++); }
@@ -1886,7 +1893,19 @@ static void simulate(dms_oracle* o, sim_t* s, const event_t* ic, dms_traj_record
 				flags |= DMS_REC_REFLECTED;
 				event_t fin = cur;
 				if(hyperbolic_kepler_shift(&fin, DMS_AU_KM))
+				{
 					flags |= DMS_REC_REFLECT_SHIFT_OK;
+					if(o->reflection != NULL)
+					{
+						/* src/Data_Generation.cpp:829-840: the speed at 1 AU and the angle of the
+						 * position to the Sun's velocity that Isoreflection_Ring bins */
+						const double* vs = o->vel_obs.x;
+						const double sun = sqrt(vs[0] * vs[0] + vs[1] * vs[1] + vs[2] * vs[2]);
+						o->reflection[0] = ev_speed(&fin);
+						o->reflection[1] = (fin.position.x[0] * vs[0] + fin.position.x[1] * vs[1] + fin.position.x[2] * vs[2]) /
+						                   ev_radius(&fin) / sun;
+					}
+				}
 			}
 		}
 	}
@@ -2082,6 +2101,41 @@ int dms_oracle_rate_grid(const dms_oracle* o, double* grid)
 	return DMS_OK;
 }
 
+/* dms_oracle_run_records in Parameter-point mode that also returns, per trajectory, the
+ * reflection-spectrum sample: reflection[2k] = speed at 1 AU [km/s], reflection[2k+1] = cosine
+ * of the angle between the position at 1 AU and the Sun's velocity; NaN unless trajectory k is a
+ * reflected particle whose final Kepler shift succeeded (src/Data_Generation.cpp:824-846). */
+int dms_oracle_run_reflections(dms_oracle* o, uint32_t seed, uint32_t point, uint64_t max_scatterings, double boundary_rsun,
+                               uint64_t first, uint64_t count, dms_traj_record* records, double* reflection)
+{
+	if(!o)
+		return DMS_ERR_INVALID_ARGUMENT;
+	o->reflection_base = reflection;
+	const int rc = dms_oracle_run_records(o, seed, point, 0, max_scatterings, boundary_rsun, first, count, records, NULL, NULL,
+	                                      NULL, 0, NULL);
+	o->reflection_base = NULL;
+	o->reflection = NULL;
+	return rc;
+}
+
+/* dms_oracle_run_records with the event after the initial Kepler shift of every trajectory
+ * given by the caller (starts: 7 doubles t [s], x [km], v [km/s] per trajectory): the initial
+ * conditions still run, so the draws after them are the usual ones.  Replays the reference's own
+ * shifted initial states (whose computation from 1000 AU amplifies last-bit differences about
+ * 1e7-fold) to compare the rest of the path. */
+int dms_oracle_run_from_starts(dms_oracle* o, uint32_t seed, uint32_t point, int capture_mode, uint64_t max_scatterings,
+                               double boundary_rsun, uint64_t first, uint64_t count, const double* starts,
+                               dms_traj_record* records, double* trace, size_t trace_capacity, size_t* trace_length)
+{
+	if(!o || !starts)
+		return DMS_ERR_INVALID_ARGUMENT;
+	o->start_base = starts;
+	const int rc = dms_oracle_run_records(o, seed, point, capture_mode, max_scatterings, boundary_rsun, first, count, records, NULL,
+	                                      NULL, trace, trace_capacity, trace_length);
+	o->start_base = NULL;
+	return rc;
+}
+
 /* Replaces the current point's N x N grid (the rate_grid member of Solar_Model,
  * include/Solar_Model.hpp:309) by one built elsewhere: the test of the engine's own device-built
  * grid replays the oracle on that grid, the same role dms_set_rate_grid plays for the engine. */
@@ -2122,12 +2176,25 @@ int dms_oracle_run_records(dms_oracle* o, uint32_t seed, uint32_t point, int cap
 		o->traj = first + k;
 		o->draw_index = 0;
 		o->trace = (trace != NULL && k == 0) ? trace : NULL;
+		o->reflection = o->reflection_base != NULL ? o->reflection_base + 2 * k : NULL;
+		if(o->reflection != NULL)
+			o->reflection[0] = o->reflection[1] = NAN;
 		o->trace_capacity = trace_capacity;
 		o->trace_length = 0;
 		DMS_OPS_MARK(3);
 		DMS_OPS_PHASE(3);
 		event_t ic = initial_conditions(o);
 		const int shift_ok = hyperbolic_kepler_shift(&ic, s.max_distance);
+		if(o->start_base != NULL)
+		{
+			const double* st = o->start_base + 7 * k;
+			ic.time = st[0];
+			for(int i = 0; i < 3; i++)
+			{
+				ic.position.x[i] = st[1 + i];
+				ic.velocity.x[i] = st[4 + i];
+			}
+		}
 		rec->initial_time = ic.time;
 		memcpy(rec->initial_position, ic.position.x, sizeof ic.position.x);
 		memcpy(rec->initial_velocity, ic.velocity.x, sizeof ic.velocity.x);

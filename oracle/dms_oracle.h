@@ -42,6 +42,17 @@ int dms_oracle_rate_grid(const dms_oracle* o, double* grid);
 /* Replaces the current point's grid by n*n values (n must equal its interpolation_points). */
 int dms_oracle_set_rate_grid(dms_oracle* o, const double* grid, uint32_t n);
 
+/* Records plus the reflection-spectrum sample per trajectory (speed at 1 AU, cosine to the Sun's
+ * velocity; NaN unless a recorded reflection), Parameter-point mode. */
+int dms_oracle_run_reflections(dms_oracle* o, uint32_t seed, uint32_t point, uint64_t max_scatterings, double boundary_rsun,
+                               uint64_t first, uint64_t count, dms_traj_record* records, double* reflection);
+
+/* Records of trajectories started from caller-given events after the initial Kepler shift
+ * (7 doubles per trajectory: t, x, v); the initial conditions still run for their draws. */
+int dms_oracle_run_from_starts(dms_oracle* o, uint32_t seed, uint32_t point, int capture_mode, uint64_t max_scatterings,
+                               double boundary_rsun, uint64_t first, uint64_t count, const double* starts,
+                               dms_traj_record* records, double* trace, size_t trace_capacity, size_t* trace_length);
+
 int dms_oracle_run_records(dms_oracle* o, uint32_t seed, uint32_t point, int capture_mode, uint64_t max_scatterings,
                            double boundary_rsun, uint64_t first, uint64_t count, dms_traj_record* records, double* hist_dt,
                            double* hist_v2dt, double* trace, size_t trace_capacity, size_t* trace_length);

@@ -22,6 +22,7 @@
 #include "Simulation_Trajectory.hpp"
 #include "Simulation_Utilities.hpp"
 #include "Solar_Model.hpp"
+#include "obscura/Astronomy.hpp"
 #include "obscura/DM_Halo_Models.hpp"
 #include "obscura/DM_Particle_Standard.hpp"
 
@@ -145,12 +146,47 @@ double dms_ref_query(int what, double a, double b, double c)
 	}
 }
 
+}	// extern "C"
+
+namespace
+{
+int Run_Records(uint32_t seed, uint32_t point, int capture_mode, uint64_t max_scatterings, double boundary_rsun, uint64_t first,
+                uint64_t count, dms_traj_record* records, double* hist_dt, double* hist_v2dt, double* trace,
+                size_t trace_capacity, size_t* trace_length, double* reflection);
+}
+
+extern "C" {
+
 // One record per trajectory id in [first, first + count).  Optional per-trajectory histograms
 // (count * NUM_BINS each) and a scatter trace of the FIRST trajectory: (r_km, v_kms, draw index)
 // per scattering, up to trace_capacity triples.
 int dms_ref_run_records(uint32_t seed, uint32_t point, int capture_mode, uint64_t max_scatterings, double boundary_rsun,
                         uint64_t first, uint64_t count, dms_traj_record* records, double* hist_dt, double* hist_v2dt,
                         double* trace, size_t trace_capacity, size_t* trace_length)
+{
+	return Run_Records(seed, point, capture_mode, max_scatterings, boundary_rsun, first, count, records, hist_dt, hist_v2dt,
+	                   trace, trace_capacity, trace_length, nullptr);
+}
+
+// The records, and for every reflected particle whose final Kepler shift to 1 AU succeeded the
+// reflection-spectrum sample of src/Data_Generation.cpp:824-840: reflection[2k] = its speed at
+// 1 AU [km/s], reflection[2k+1] = the cosine of the angle between its position at 1 AU and the
+// Sun's velocity (the quantity Isoreflection_Ring bins, src/Simulation_Utilities.cpp:82-92);
+// NaN for every other trajectory.
+int dms_ref_run_reflections(uint32_t seed, uint32_t point, uint64_t max_scatterings, double boundary_rsun, uint64_t first,
+                            uint64_t count, dms_traj_record* records, double* reflection)
+{
+	return Run_Records(seed, point, 0, max_scatterings, boundary_rsun, first, count, records, nullptr, nullptr, nullptr, 0,
+	                   nullptr, reflection);
+}
+
+}	// extern "C"
+
+namespace
+{
+int Run_Records(uint32_t seed, uint32_t point, int capture_mode, uint64_t max_scatterings, double boundary_rsun, uint64_t first,
+                uint64_t count, dms_traj_record* records, double* hist_dt, double* hist_v2dt, double* trace,
+                size_t trace_capacity, size_t* trace_length, double* reflection)
 {
 	if(!g_ssm || !g_dm || !g_halo)
 		return -1;
@@ -168,6 +204,8 @@ int dms_ref_run_records(uint32_t seed, uint32_t point, int capture_mode, uint64_
 			std::memset(&rec, 0, sizeof(rec));
 			rec.trajectory_id = id;
 			rec.point = point;
+			if(reflection)
+				reflection[2 * k] = reflection[2 * k + 1] = std::numeric_limits<double>::quiet_NaN();
 			Event IC = Initial_Conditions(*g_halo, *g_ssm, simulator.PRNG);
 			const bool shift_ok = Hyperbolic_Kepler_Shift(IC, R);
 			To_Engine(IC, rec.initial_time, rec.initial_position, rec.initial_velocity);
@@ -206,7 +244,15 @@ int dms_ref_run_records(uint32_t seed, uint32_t point, int capture_mode, uint64_
 					flags |= DMS_REC_REFLECTED;
 					Event final_event = result.final_event;
 					if(Hyperbolic_Kepler_Shift(final_event, 1.0 * AU))
+					{
 						flags |= DMS_REC_REFLECT_SHIFT_OK;
+						if(reflection)
+						{
+							const libphysica::Vector vs = obscura::Sun_Velocity();
+							reflection[2 * k] = In_Units(final_event.Speed(), km / sec);
+							reflection[2 * k + 1] = final_event.position.Dot(vs) / final_event.position.Norm() / vs.Norm();
+						}
+					}
 				}
 			}
 			rec.flags = flags;
@@ -249,6 +295,9 @@ int dms_ref_run_records(uint32_t seed, uint32_t point, int capture_mode, uint64_
 		return -1;
 	}
 }
+}	// namespace
+
+extern "C" {
 
 // The reference's own ensemble driver, Simulation_Data::Generate_Data + output writers, on one
 // process (single-rank MPI shim).  Draws come from one sequential stream keyed by (seed, point).

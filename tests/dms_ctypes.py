@@ -86,6 +86,13 @@ class Oracle:
         lib.dms_oracle_tables.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 6
         lib.dms_oracle_rate_grid.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         lib.dms_oracle_set_rate_grid.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]
+        lib.dms_oracle_run_from_starts.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                                   ctypes.c_uint64, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64,
+                                                   ctypes.c_void_p, ctypes.POINTER(TrajRecord), ctypes.c_void_p,
+                                                   ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+        lib.dms_oracle_run_reflections.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                                   ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64,
+                                                   ctypes.POINTER(TrajRecord), ctypes.c_void_p]
         lib.dms_oracle_run_records.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
                                                ctypes.c_uint64, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64,
                                                ctypes.POINTER(TrajRecord), ctypes.c_void_p, ctypes.c_void_p,
@@ -126,6 +133,38 @@ class Oracle:
         g = np.zeros(self.point_n * self.point_n)
         self.lib.dms_oracle_rate_grid(self.h, g.ctypes.data)
         return g.reshape(self.point_n, self.point_n)
+
+    def run_reflections(self, seed, point, first, count, max_scatterings=10**6, boundary_rsun=2.0):
+        """Records and the per-trajectory reflection-spectrum sample (speed at 1 AU, cosine to the
+        Sun's velocity; NaN unless a recorded reflection), Parameter-point mode."""
+        import numpy as np
+        recs = (TrajRecord * count)()
+        out = np.zeros((count, 2))
+        rc = self.lib.dms_oracle_run_reflections(self.h, seed, point, max_scatterings, boundary_rsun, first, count, recs,
+                                                 out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("oracle run_reflections failed %d" % rc)
+        return recs, out
+
+    def run_from_starts(self, seed, point, first, starts, capture_mode=False, max_scatterings=10**6, boundary_rsun=2.0,
+                        trace_capacity=0):
+        """Records of ids [first, first + len(starts)) started from the given events after the
+        initial Kepler shift (rows t, x, v; e.g. the reference's own), with the usual draws."""
+        import numpy as np
+        st = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 7)
+        count = len(st)
+        recs = (TrajRecord * count)()
+        tr = np.zeros((max(trace_capacity, 1), 3)) if trace_capacity else None
+        tl = ctypes.c_size_t(0)
+        rc = self.lib.dms_oracle_run_from_starts(self.h, seed, point, int(capture_mode), max_scatterings, boundary_rsun, first,
+                                                 count, st.ctypes.data, recs, tr.ctypes.data if tr is not None else None,
+                                                 trace_capacity, ctypes.byref(tl))
+        if rc != 0:
+            raise RuntimeError("oracle run_from_starts failed %d" % rc)
+        out = {"records": recs}
+        if trace_capacity:
+            out["trace"] = tr[: min(tl.value, trace_capacity)]
+        return out
 
     def set_rate_grid(self, grid):
         """Replays on a grid built elsewhere (e.g. the engine's device-built grid)."""
@@ -172,6 +211,8 @@ class Reference:
                                             ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64,
                                             ctypes.POINTER(TrajRecord), ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+        lib.dms_ref_run_reflections.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double,
+                                                ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(TrajRecord), ctypes.c_void_p]
         lib.dms_ref_generate_data.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint32,
                                               ctypes.c_uint32, ctypes.c_uint64, ctypes.c_char_p]
         lib.dms_ref_last_error.restype = ctypes.c_char_p
@@ -207,3 +248,16 @@ class Reference:
         if trace_capacity:
             out["trace"] = tr[: min(tl.value, trace_capacity)]
         return out
+
+    def run_reflections(self, seed, point, first, count, max_scatterings=10**6, boundary_rsun=2.0):
+        """Records of ids [first, first + count) in Parameter-point mode and, per trajectory, the
+        reflection-spectrum sample (speed at 1 AU [km/s], cosine to the Sun's velocity; NaN when the
+        trajectory is not a recorded reflection)."""
+        import numpy as np
+        recs = (TrajRecord * count)()
+        out = np.zeros((count, 2))
+        rc = self.lib.dms_ref_run_reflections(seed, point, max_scatterings, boundary_rsun, first, count, recs,
+                                              out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("reference run_reflections failed: %s" % self.lib.dms_ref_last_error())
+        return recs, out

@@ -82,6 +82,38 @@ def test_first_scattering_agrees(oracle_golden_point, golden, mode):
     assert errs and max(errs) < 1e-7 and float(np.median(errs)) < 1e-10
 
 
+@pytest.mark.parametrize("mode", ["normal", "capture"])
+def test_replay_from_the_reference_initial_states(oracle_golden_point, golden, mode):
+    """The path after the initial conditions, pinned separately.  The map from the halo sample at
+    1000 AU to the event at 2 R_sun (Initial_Conditions + Hyperbolic_Kepler_Shift,
+    src/Simulation_Utilities.cpp:176-321) amplifies last-bit differences about 1e7-fold, so the
+    oracle's own initial states (km units, the shared series for sin/cos/acos) differ from the
+    reference's (natural units, glibc) by about 1e-9 relative.  Started from the reference's own
+    shifted states (the fixture's "initial"), the oracle reproduces the outcomes of (nearly)
+    every trajectory, and the first scatterings agree to 1e-10 for most of them; the rest differ
+    because the RK45 step-size control divides the tolerance by |r5 - r4|, a cancellation whose
+    last bits differ between unit systems, so step sequences carry rounding noise
+    (src/Simulation_Trajectory.cpp:477-502, 1540-1545)."""
+    from dms_ctypes import records_to_dicts
+    import numpy as np
+    ref = golden["modes"][mode]["records"]
+    starts = np.array([[r["initial"][0]] + list(r["initial"][1]) + list(r["initial"][2]) for r in ref])
+    capture = mode == "capture"
+    mine = records_to_dicts(oracle_golden_point.run_from_starts(golden["seed"], 0, 0, starts, capture_mode=capture)["records"])
+    same = sum(_outcome(a) == _outcome(b) for a, b in zip(ref, mine))
+    assert same >= (len(ref) if capture else int(math.ceil(0.99 * len(ref))))
+    errs = []
+    for t, ref_tr in enumerate(golden["modes"][mode]["first_scatter"]):
+        if ref_tr is None:
+            continue
+        tr = oracle_golden_point.run_from_starts(golden["seed"], 0, t, starts[t:t + 1], capture_mode=capture,
+                                                 trace_capacity=1)["trace"]
+        assert tr[0][2] == ref_tr[2]
+        errs.append(max(abs(tr[0][0] - ref_tr[0]) / ref_tr[0], abs(tr[0][1] - ref_tr[1]) / ref_tr[1]))
+    errs = np.array(errs)
+    assert np.median(errs) < 2e-11 and np.mean(errs <= 1e-10) >= 0.85 and errs.max() < 1e-8
+
+
 DP_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_dark_photon.json")
 
 
