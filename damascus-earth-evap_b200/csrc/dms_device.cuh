@@ -960,6 +960,126 @@ __device__ __forceinline__ int rk45_attempt_cert(const DevSolar& S, Prop& p, int
 	return RK_RETRY;
 }
 
+// The attempt of rk45_attempt_cert computed by two lanes of a warp: an owner (role 1, the lane
+// whose propagator steps) and a helper (role 2, an idle lane), `partner` being the other lane of
+// the pair.  Every lane of the warp calls it (the exchanges are warp shuffles); lanes without a
+// pair (role 0) compute nothing that is kept.  The radius of stage j needs the slopes of the
+// stages up to j - 2 only, so the owner computes stages 0, 2, 4 and the helper 1, 3, 5, three
+// rounds instead of six, exchanging the new slopes after each round; the owner then forms the
+// solutions, the helper two of the three step-size factors.  Every value is formed by the same
+// operations in the same order as in rk45_attempt_cert, so the result is the same bits.  Only
+// the owner's p is changed; `good` (owner) is cleared when a certificate of either lane failed.
+__device__ __forceinline__ int rk45_attempt_pair(const DevSolar& S, Prop& p, int inner, int role, int partner, bool& good)
+{
+	constexpr unsigned int FULL = 0xffffffffu;
+	const int me = threadIdx.x & 31;
+	const int src = role == 2 ? partner : me;
+	Prop q = p;
+	q.time_step = __shfl_sync(FULL, p.time_step, src);
+	q.radius = __shfl_sync(FULL, p.radius, src);
+	q.v_radial = __shfl_sync(FULL, p.v_radial, src);
+	q.J = __shfl_sync(FULL, p.J, src);
+	q.radial_mode = __shfl_sync(FULL, p.radial_mode, src);
+	const bool odd = role == 2;
+	const int other = role == 0 ? me : partner;
+	const double dt = q.time_step;
+	const double R = q.radius, V = q.v_radial;
+	double a, b;
+	const double kr0 = dt * V;
+	// round 1: stage 0 (owner) | stage 1 (helper)
+	const double r_s1 = R + kr0 / 4.0;
+	cert_stage<true>(S, q, odd ? r_s1 : R, a, b, good);
+	const double kv_m1 = dt * a, kp_m1 = dt * b;
+	const double kv_o1 = __shfl_sync(FULL, kv_m1, other);
+	const double kv0 = odd ? kv_o1 : kv_m1, kv1 = odd ? kv_m1 : kv_o1;
+	const double kr1 = dt * (V + kv0 / 4.0);
+	const double kr2 = dt * (V + 3.0 / 32.0 * kv0 + 9.0 / 32.0 * kv1);
+	// round 2: stage 2 | stage 3
+	const double r_s2 = R + 3.0 / 32.0 * kr0 + 9.0 / 32.0 * kr1;
+	const double r_s3 = R + 1932.0 / 2197.0 * kr0 - 7200.0 / 2197.0 * kr1 + 7296.0 / 2197.0 * kr2;
+	cert_stage<true>(S, q, odd ? r_s3 : r_s2, a, b, good);
+	const double kv_m2 = dt * a, kp_m2 = dt * b;
+	const double kv_o2 = __shfl_sync(FULL, kv_m2, other);
+	const double kv2 = odd ? kv_o2 : kv_m2, kv3 = odd ? kv_m2 : kv_o2;
+	const double kr3 = dt * (V + 1932.0 / 2197.0 * kv0 - 7200.0 / 2197.0 * kv1 + 7296.0 / 2197.0 * kv2);
+	const double kr4 = dt * (V + 439.0 / 216.0 * kv0 - 8.0 * kv1 + 3680.0 / 513.0 * kv2 - 845.0 / 4104.0 * kv3);
+	// round 3: stage 4 | stage 5
+	const double r_s4 = R + 439.0 / 216.0 * kr0 - 8.0 * kr1 + 3680.0 / 513.0 * kr2 - 845.0 / 4104.0 * kr3;
+	const double r_s5 = R - 8.0 / 27.0 * kr0 + 2.0 * kr1 - 3544.0 / 2565.0 * kr2 + 1859.0 / 4104.0 * kr3 - 11.0 / 40.0 * kr4;
+	cert_stage<true>(S, q, odd ? r_s5 : r_s4, a, b, good);
+	const double kv_m3 = dt * a, kp_m3 = dt * b;
+	// both lanes gather every slope: the owner's kp of rounds 1-3 are kp0, kp2, kp4, the
+	// helper's kp3, kp5 (its round-1 dphi belongs to stage 1, which has none)
+	const double kv_o3 = __shfl_sync(FULL, kv_m3, other);
+	const double kp_o1 = __shfl_sync(FULL, kp_m1, other);
+	const double kp_o2 = __shfl_sync(FULL, kp_m2, other);
+	const double kp_o3 = __shfl_sync(FULL, kp_m3, other);
+	const double kv4 = odd ? kv_o3 : kv_m3, kv5 = odd ? kv_m3 : kv_o3;
+	const double kp0 = odd ? kp_o1 : kp_m1;
+	const double kp2 = odd ? kp_o2 : kp_m2, kp3 = odd ? kp_m2 : kp_o2;
+	const double kp4 = odd ? kp_o3 : kp_m3, kp5 = odd ? kp_m3 : kp_o3;
+	const double kr5 = dt * (V - 8.0 / 27.0 * kv0 + 2.0 * kv1 - 3544.0 / 2565.0 * kv2 + 1859.0 / 4104.0 * kv3 - 11.0 / 40.0 * kv4);
+	const double r4 = R + 25.0 / 216.0 * kr0 + 1408.0 / 2565.0 * kr2 + 2197.0 / 4104.0 * kr3 - 1.0 / 5.0 * kr4;
+	const double v4 = V + 25.0 / 216.0 * kv0 + 1408.0 / 2565.0 * kv2 + 2197.0 / 4104.0 * kv3 - 1.0 / 5.0 * kv4;
+	const double p4 = p.phi + 25.0 / 216.0 * kp0 + 1408.0 / 2565.0 * kp2 + 2197.0 / 4104.0 * kp3 - 1.0 / 5.0 * kp4;
+	const double r5 = R + 16.0 / 135.0 * kr0 + 6656.0 / 12825.0 * kr2 + 28561.0 / 56430.0 * kr3 - 9.0 / 50.0 * kr4 + 2.0 / 55.0 * kr5;
+	const double v5 = V + 16.0 / 135.0 * kv0 + 6656.0 / 12825.0 * kv2 + 28561.0 / 56430.0 * kv3 - 9.0 / 50.0 * kv4 + 2.0 / 55.0 * kv5;
+	const double p5 = p.phi + 16.0 / 135.0 * kp0 + 6656.0 / 12825.0 * kp2 + 28561.0 / 56430.0 * kp3 - 9.0 / 50.0 * kp4 + 2.0 / 55.0 * kp5;
+	const double e0 = fabs(r5 - r4), e1 = fabs(v5 - v4), e2 = fabs(p5 - p4);
+	// the step-size factors: c0 and c2 on the owner, c1 (and c2 again) on the helper, whose e2
+	// needs the owner's phi
+	const double phi_o = __shfl_sync(FULL, p.phi, src);
+	const double p4h = phi_o + 25.0 / 216.0 * kp0 + 1408.0 / 2565.0 * kp2 + 2197.0 / 4104.0 * kp3 - 1.0 / 5.0 * kp4;
+	const double p5h = phi_o + 16.0 / 135.0 * kp0 + 6656.0 / 12825.0 * kp2 + 28561.0 / 56430.0 * kp3 - 9.0 / 50.0 * kp4 + 2.0 / 55.0 * kp5;
+	const double e2h = fabs(p5h - p4h);
+	const double cA = cert_step_factor(odd ? DMS_RK45_TOL_V_KMS : DMS_RK45_TOL_R_KM, odd ? e1 : e0, good);
+	const double cB = cert_step_factor(DMS_RK45_TOL_PHI, e2h, good);
+	const double c1 = __shfl_sync(FULL, cA, other), c2 = cB;
+	const int helper_good = __shfl_sync(FULL, static_cast<int>(good), other);
+	if(role != 1)
+		return RK_RETRY;
+	good = good && helper_good != 0;
+	const double c0 = cA;
+	double factor = DMS_RK45_MAX_STEP_FACTOR;
+	factor = c0 < factor ? c0 : factor;
+	factor = c1 < factor ? c1 : factor;
+	factor = c2 < factor ? c2 : factor;
+	factor = factor > DMS_RK45_MAX_STEP_FACTOR ? DMS_RK45_MAX_STEP_FACTOR : factor;
+	factor = factor < DMS_RK45_MIN_STEP_FACTOR ? DMS_RK45_MIN_STEP_FACTOR : factor;
+	const double grown = factor * dt;
+	const double sane = (!isfinite(grown) | (grown <= 0.0)) ? DMS_RK45_DEFAULT_STEP_S
+	                    : (grown < DMS_RK45_ABS_MAX_STEP_S ? grown : DMS_RK45_ABS_MAX_STEP_S);
+	const bool finite_err = isfinite(e0) & isfinite(e1) & isfinite(e2);
+	const double new_step = finite_err ? sane : DMS_RK45_MIN_STEP_FACTOR * dt;
+	const bool within = finite_err & (e0 <= DMS_RK45_TOL_R_KM) & (e1 <= DMS_RK45_TOL_V_KMS) & (e2 <= DMS_RK45_TOL_PHI);
+	if(!good)
+		return RK_RETRY;
+	if(within)
+	{
+		p.time = p.time + dt;
+		p.radius = r4 < 0.0 ? 0.0 : r4;
+		p.v_radial = v4;
+		p.phi = p4;
+		p.time_step = new_step;
+		return RK_ACCEPTED;
+	}
+	if(new_step < DMS_RK45_ABS_MIN_STEP_S || inner >= DMS_RK45_MAX_INNER_RETRIES)
+	{
+		const bool ok = isfinite(r4) && isfinite(v4) && isfinite(p4);
+		p.time = p.time + DMS_RK45_ABS_MIN_STEP_S;
+		if(ok)
+		{
+			p.radius = r4 < 0.0 ? 0.0 : r4;
+			p.v_radial = v4;
+			p.phi = p4;
+		}
+		p.time_step = DMS_RK45_ABS_MIN_STEP_S;
+		return RK_FORCED;
+	}
+	p.time_step = new_step;
+	return RK_RETRY;
+}
+
 // One attempt with the certified straight-line division and square root; when any certificate
 // fails (or the tables' buckets can hold two knots), the attempt is repeated from the same
 // state with IEEE arithmetic.  Either way the result is bit-identical with rk45_attempt_unrolled.

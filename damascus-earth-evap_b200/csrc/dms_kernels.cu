@@ -69,10 +69,10 @@ __device__ __forceinline__ double commit_event(const DevSolar& S, double m_dm, i
 
 // One pass of the Propagate_Freely loop body, src/Simulation_Trajectory.cpp:876-1116, split at the
 // RK45 retry loop: when no step is in progress the pre-step bounds are applied and a step is
-// opened; every pass makes one RK45 attempt; only a finished step runs the optical-depth,
-// boundary and commit logic.  Returns the next phase of the lane.
-__device__ __forceinline__ int free_step(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L, double2* hist,
-                                         int drained)
+// opened (free_step_begin); every pass makes one RK45 attempt; only a finished step runs the
+// optical-depth, boundary and commit logic (free_step_finish).  free_step_begin returns PH_STEP
+// when an attempt is due, else the lane's next phase.
+__device__ __forceinline__ int free_step_begin(const RunParams& R, const DevPoint* __restrict__ P, StrictLane& L)
 {
 	const DevSolar& S = R.S;
 	const int capture_mode = R.capture_mode;
@@ -135,14 +135,32 @@ __device__ __forceinline__ int free_step(const RunParams& R, const DevPoint* __r
 		L.in_rk = 1;
 		L.rk_inner = 0;
 	}
+	return PH_STEP;
+}
+
+// One RK45 attempt of the lane's open step (the lane alone).
+__device__ __forceinline__ int free_step_attempt(const DevSolar& S, StrictLane& L, int drained)
+{
 	L.rk_inner++;
 #if DMS_RK_UNROLLED == 2
-	const int rk = drained ? rk45_attempt_written_out(S, L.pr, L.rk_inner) : rk45_attempt(S, L.pr, L.rk_inner);
+	return drained ? rk45_attempt_written_out(S, L.pr, L.rk_inner) : rk45_attempt(S, L.pr, L.rk_inner);
 #elif DMS_RK_UNROLLED == 1
-	const int rk = rk45_attempt_written_out(S, L.pr, L.rk_inner);
+	(void)drained;
+	return rk45_attempt_written_out(S, L.pr, L.rk_inner);
 #else
-	const int rk = rk45_attempt(S, L.pr, L.rk_inner);
+	(void)drained;
+	return rk45_attempt(S, L.pr, L.rk_inner);
 #endif
+}
+
+// The rest of the pass after an attempt with result rk: a retry keeps the step open; a
+// finished step runs the optical-depth, boundary and commit logic.
+__device__ __forceinline__ int free_step_finish(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L,
+                                                double2* hist, int rk)
+{
+	const DevSolar& S = R.S;
+	const int capture_mode = R.capture_mode;
+	const double tau_limit = capture_mode ? DMS_CAPTURE_MAX_OPTICAL_DEPTH_STEP : DMS_MAX_OPTICAL_DEPTH_STEP;
 	if(rk == RK_RETRY)
 		return PH_STEP;
 	L.in_rk = 0;
@@ -399,10 +417,40 @@ __global__ void __launch_bounds__(128) initial_state_kernel(const RunParams R)
 
 struct StrictStep
 {
+	// the lane loop runs a step as begin / attempt / finish and may pair the attempt of a lane
+	// with an idle lane of its warp (rk45_attempt_pair)
+	static constexpr bool pairs = DMS_PAIRED_ATTEMPTS != 0 && DMS_CERTIFIED_MATH != 0 && DMS_RK_UNROLLED == 1;
+	__device__ __forceinline__ int begin(const RunParams& R, const DevPoint* __restrict__ P, StrictLane& L) const
+	{
+		return free_step_begin(R, P, L);
+	}
+	__device__ __forceinline__ int attempt(const DevSolar& S, StrictLane& L, int drained) const
+	{
+		return free_step_attempt(S, L, drained);
+	}
+	// all lanes of the warp call this; role 1 = owner (its attempt), 2 = helper, 0 = neither
+	__device__ __forceinline__ int pair_attempt(const DevSolar& S, StrictLane& L, int role, int partner) const
+	{
+		if(role == 1)
+			L.rk_inner++;
+		bool good = S.bucket_single_step != 0;
+		const int rk = rk45_attempt_pair(S, L.pr, L.rk_inner, role, partner, good);
+		if(role == 1 && !good)
+			return rk45_attempt_ieee(S, L.pr, L.rk_inner);
+		return rk;
+	}
+	__device__ __forceinline__ int finish(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L, double2* hist,
+	                                      int rk) const
+	{
+		return free_step_finish(R, P, m_dm, L, hist, rk);
+	}
 	__device__ __forceinline__ int operator()(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L, double2* hist,
 	                                          int drained) const
 	{
-		return free_step(R, P, m_dm, L, hist, drained);
+		const int ph = begin(R, P, L);
+		if(ph != PH_STEP)
+			return ph;
+		return finish(R, P, m_dm, L, hist, attempt(R.S, L, drained));
 	}
 	__device__ __forceinline__ double channel(const DevSolar& S, const DevPoint* __restrict__ P, int i, double dr, double T, double v, int k) const
 	{

@@ -25,6 +25,20 @@
 #ifndef DMS_CERTIFIED_MATH
 #define DMS_CERTIFIED_MATH 1
 #endif
+// FP64 attempts of lanes that run with idle lanes beside them are computed by two lanes
+// (rk45_attempt_pair) when 1; always by the lane alone when 0.  The same bits either way.
+#ifndef DMS_PAIRED_ATTEMPTS
+#define DMS_PAIRED_ATTEMPTS 1
+#endif
+// Pairing applies to warps with at most DMS_PAIR_MAX_LANES attempting lanes (up to 16, every
+// one paired with an idle lane) and, when DMS_PAIR_ONLY_DRAINED, only once the block has seen
+// the work queue drained (the tail of a launch).
+#ifndef DMS_PAIR_MAX_LANES
+#define DMS_PAIR_MAX_LANES 16
+#endif
+#ifndef DMS_PAIR_ONLY_DRAINED
+#define DMS_PAIR_ONLY_DRAINED 1
+#endif
 #ifndef DMS_RK_UNROLLED_MIXED
 #define DMS_RK_UNROLLED_MIXED 1
 #endif

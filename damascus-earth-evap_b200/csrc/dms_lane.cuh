@@ -666,6 +666,13 @@ __device__ __forceinline__ int finish_scatter(const RunParams& R, const DevPoint
 }
 
 
+// Position of the (n+1)-th set bit of m (n from 0); m must have more than n set bits.
+__device__ __forceinline__ int nth_set_bit(unsigned int m, int n)
+{
+	for(int t = 0; t < n; t++) m &= m - 1u;
+	return __ffs(m) - 1;
+}
+
 template <class Lane, class Step>
 __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 {
@@ -753,7 +760,50 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 		}
 		if(phase == PH_SEGMENT)
 			phase = segment_start(R, P, m_dm, L);
-		if(phase == PH_STEP)
+		if constexpr(Step::pairs)
+		{
+			// A step is opened per lane; its RK45 attempt then runs paired when at most half of
+			// the warp is attempting: every attempting lane takes an idle lane of its warp as a
+			// helper for the independent stages (rk45_attempt_pair), which shortens the dependent
+			// chain of a lane that runs alone, the tail of a launch.  Same results either way.
+			const int drained = *reinterpret_cast<volatile int*>(&queue_drained);
+			bool want = false;
+			if(phase == PH_STEP)
+			{
+				const int ph = step.begin(R, P, L);
+				want = ph == PH_STEP;
+				if(!want)
+					phase = ph;
+			}
+			const unsigned int att = __ballot_sync(FULL_WARP, want);
+			const int n_att = __popc(att);
+			if(n_att != 0 && n_att <= DMS_PAIR_MAX_LANES && (drained || !DMS_PAIR_ONLY_DRAINED))
+			{
+				const int me = threadIdx.x & 31;
+				int role = 0, partner = me;
+				const unsigned int below = lane_bit - 1u;
+				if(want)
+				{
+					role = 1;
+					partner = nth_set_bit(~att, __popc(att & below));
+				}
+				else
+				{
+					const int q = __popc(~att & below);
+					if(q < n_att)
+					{
+						role = 2;
+						partner = nth_set_bit(att, q);
+					}
+				}
+				const int rk = step.pair_attempt(R.S, L, role, partner);
+				if(want)
+					phase = step.finish(R, P, m_dm, L, hist, rk);
+			}
+			else if(want)
+				phase = step.finish(R, P, m_dm, L, hist, step.attempt(R.S, L, drained));
+		}
+		else if(phase == PH_STEP)
 			phase = step(R, P, m_dm, L, hist, *reinterpret_cast<volatile int*>(&queue_drained));
 		// Scatterings wait until several lanes of the warp have one (or one has waited
 		// R.scatter_wait iterations, or no lane is stepping), so that the scattering code
