@@ -419,7 +419,7 @@ struct StrictStep
 {
 	// the lane loop runs a step as begin / attempt / finish and may pair the attempt of a lane
 	// with an idle lane of its warp (rk45_attempt_pair)
-	static constexpr bool pairs = DMS_PAIRED_ATTEMPTS != 0 && DMS_CERTIFIED_MATH != 0 && DMS_RK_UNROLLED == 1;
+	static constexpr bool pairs = DMS_PAIRED_ATTEMPTS != 0 && DMS_CERTIFIED_MATH != 0 && DMS_RK_UNROLLED >= 1;
 	__device__ __forceinline__ int begin(const RunParams& R, const DevPoint* __restrict__ P, StrictLane& L) const
 	{
 		return free_step_begin(R, P, L);

@@ -14,11 +14,11 @@
 // instruction-cache misses with every lane busy), 1 = the stages written out (a shorter
 // dependent chain for a lane that runs alone), 2 = the loop while the work queue still has
 // items and the written-out stages once the block has seen it drained (a lane's fetch, or the
-// queue head read every 64 iterations).  Form 2 is measured 10 % faster with every lane busy
-// and 8 % faster in Capture mode; the default stays 1 because the bench step is bounded by its
-// tail, which form 2 does not shorten.
+// queue head read every 64 iterations).  With the FP64 tail attempts paired across two lanes
+// (DMS_PAIRED_ATTEMPTS), form 2 is the default: measured 13 % more accepted steps per second
+// with every lane busy than form 1, the same time per step for a lane that runs alone.
 #ifndef DMS_RK_UNROLLED
-#define DMS_RK_UNROLLED 1
+#define DMS_RK_UNROLLED 2
 #endif
 // FP64 RK45 attempts with the certified straight-line division and square root of
 // dms_fastmath.cuh (1) or with IEEE `/` and sqrt (0); the results are the same bits.
