@@ -79,6 +79,10 @@ __device__ __forceinline__ int free_step_begin(const RunParams& R, const DevPoin
 	const double tau_limit = capture_mode ? DMS_CAPTURE_MAX_OPTICAL_DEPTH_STEP : DMS_MAX_OPTICAL_DEPTH_STEP;
 	if(!L.in_rk)
 	{
+		// speed and rate at the propagator's state, formed by the previous step's finish (tail of
+		// a launch) from the same propagator
+		const bool cached = L.next_valid != 0;
+		L.next_valid = 0;
 		if(!(L.seg_steps < R.max_free_steps))
 		{
 			L.reason = DMS_REASON_MAX_FREE_STEPS;  // L.cur holds the last committed event
@@ -95,7 +99,7 @@ __device__ __forceinline__ int free_step_begin(const RunParams& R, const DevPoin
 			L.before_valid = 1;
 		}
 		const double r_before = prop_radius(L.pr);
-		const double v_before = prop_speed(L.pr);
+		const double v_before = cached ? L.next_speed : prop_speed(L.pr);
 		L.rate_before = 0.0;
 		if(r_before >= DMS_RSUN_KM)
 		{
@@ -116,7 +120,7 @@ __device__ __forceinline__ int free_step_begin(const RunParams& R, const DevPoin
 		else
 		{
 			L.pr.time_step = sanitized_step(L.pr.time_step);
-			L.rate_before = rate_total(S, P, r_before, v_before);
+			L.rate_before = cached ? L.next_rate : rate_total(S, P, r_before, v_before);
 			if(!isfinite(L.rate_before) || L.rate_before < 0.0)
 			{
 				set_final(L, prop_event(L.pr), true, DMS_REASON_NUMERICAL_FAILURE);
@@ -155,98 +159,107 @@ __device__ __forceinline__ int free_step_attempt(const DevSolar& S, StrictLane& 
 
 // The rest of the pass after an attempt with result rk: a retry keeps the step open; a
 // finished step runs the optical-depth, boundary and commit logic.
-__device__ __forceinline__ int free_step_finish(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L,
-                                                double2* hist, int rk)
+// The trapezoid sums of the depth loop in free_step_finish over rates that are already formed:
+// the same additions in the same order.
+template <int PIECES>
+__device__ __forceinline__ void depth_sums(const double (&fr)[DMS_MAX_OPTICAL_DEPTH_PIECES + 1], const double (&rt)[DMS_MAX_OPTICAL_DEPTH_PIECES + 1],
+                                           double actual_dt, double& dtau, double& tau2, bool& invalid)
 {
-	const DevSolar& S = R.S;
-	const int capture_mode = R.capture_mode;
-	const double tau_limit = capture_mode ? DMS_CAPTURE_MAX_OPTICAL_DEPTH_STEP : DMS_MAX_OPTICAL_DEPTH_STEP;
+	double tau2_a = 0.0;
+#pragma unroll
+	for(int i = 0; i <= PIECES; i++)
+	{
+		const double f = fr[i], rate = rt[i];
+		if(!isfinite(rate) || rate < 0.0)
+			invalid = true;
+		if(i > 0 && f > fr[i - 1])
+			dtau += 0.5 * (rt[i - 1] + rate) * (actual_dt * (f - fr[i - 1]));
+		if(PIECES >= 4)
+		{
+			if(i == 2)
+				tau2_a = 0.5 * (rt[0] + rt[2]) * (actual_dt * (fr[2] - fr[0]));
+			else if(i == 4)
+				tau2 = tau2_a + 0.5 * (rt[2] + rate) * (actual_dt * (f - fr[2]));
+		}
+		else if(i > 0)
+			tau2 += 0.5 * (rt[i - 1] + rate) * (actual_dt * (f - fr[i - 1]));
+	}
+}
+
+// A finished RK45 step as the head of free_step_finish leaves it for the tail: the events and
+// radii before and after it and its interior interval.
+struct FinishCtx
+{
+	Event before, after;
+	double r_before, rate_before, actual_dt, r_after, v_after, s0, s1;
+	int interior;  // the chord enters the Sun (interior_interval)
+	int depth;     // with a positive span and duration: the piece rates are formed
+};
+
+constexpr int PH_CONTINUE = -1;  // free_step_finish_head: the step goes on to its tail
+
+// The checks after an attempt (src/Simulation_Trajectory.cpp:930-960) and the interior interval.
+__device__ __forceinline__ int free_step_finish_head(const RunParams& R, StrictLane& L, int rk, FinishCtx& c)
+{
 	if(rk == RK_RETRY)
 		return PH_STEP;
 	L.in_rk = 0;
 	L.attempts += static_cast<uint64_t>(L.rk_inner);
-	const Event before = L.before;
-	const double r_before = L.b_radius < 0.0 ? 0.0 : L.b_radius;
-	const double rate_before = L.rate_before;
-	const double actual_dt = L.pr.time - L.b_time;
-	const double r_after = prop_radius(L.pr);
-	const double v_after = prop_speed(L.pr);
-	const Event after = prop_event(L.pr);
+	c.before = L.before;
+	c.r_before = L.b_radius < 0.0 ? 0.0 : L.b_radius;
+	c.rate_before = L.rate_before;
+	c.actual_dt = L.pr.time - L.b_time;
+	c.r_after = prop_radius(L.pr);
+	c.v_after = prop_speed(L.pr);
+	c.after = prop_event(L.pr);
 	if(rk == RK_FORCED)
 	{
-		set_final(L, after, true, DMS_REASON_NUMERICAL_FAILURE);
+		set_final(L, c.after, true, DMS_REASON_NUMERICAL_FAILURE);
 		return PH_FINAL;
 	}
-	if(!isfinite(r_after) || !isfinite(v_after) || !isfinite(actual_dt) || actual_dt <= 0.0)
+	if(!isfinite(c.r_after) || !isfinite(c.v_after) || !isfinite(c.actual_dt) || c.actual_dt <= 0.0)
 	{
-		set_final(L, after, true, DMS_REASON_NON_FINITE_STATE);
+		set_final(L, c.after, true, DMS_REASON_NON_FINITE_STATE);
 		return PH_FINAL;
 	}
-	if(v_after > DMS_V_MAX_C * DMS_C_KMS)
+	if(c.v_after > DMS_V_MAX_C * DMS_C_KMS)
 	{
-		set_final(L, after, true, DMS_REASON_SPEED_LIMIT);
+		set_final(L, c.after, true, DMS_REASON_SPEED_LIMIT);
 		return PH_FINAL;
 	}
 	if(wall_time_exceeded(R, L))  // "after_rk45_step", src/Simulation_Trajectory.cpp:953-954
 	{
-		set_final(L, after, true, DMS_REASON_WALL_TIME_LIMIT);
+		set_final(L, c.after, true, DMS_REASON_WALL_TIME_LIMIT);
 		return PH_FINAL;
 	}
+	c.s0 = 0.0;
+	c.s1 = 0.0;
+	c.interior = interior_interval(c.before, c.after, c.r_before, c.r_after, c.s0, c.s1) ? 1 : 0;
+	c.depth = (c.interior && c.s1 > c.s0 && c.actual_dt > 0.0) ? 1 : 0;
+	return PH_CONTINUE;
+}
+
+// The optical depth, boundary and commit logic of a finished step (src/Simulation_Trajectory.cpp:
+// 960-1116) from its piece boundaries fr and rates rt, their trapezoid sums dtau (pieces) and
+// tau2 (two-piece estimate) and whether a rate was invalid.  next_ok: next_rate is the scattering
+// rate at the propagator's state (rate_total at r_after, v_after), for the next step's head.
+__device__ __forceinline__ int free_step_finish_tail(const RunParams& R, double m_dm, StrictLane& L, double2* hist,
+                                                     const FinishCtx& c, const double (&fr)[DMS_MAX_OPTICAL_DEPTH_PIECES + 1],
+                                                     const double (&rt)[DMS_MAX_OPTICAL_DEPTH_PIECES + 1], double dtau, double tau2, bool invalid,
+                                                     bool next_ok, double next_rate)
+{
+	const DevSolar& S = R.S;
+	const int capture_mode = R.capture_mode;
+	const double tau_limit = capture_mode ? DMS_CAPTURE_MAX_OPTICAL_DEPTH_STEP : DMS_MAX_OPTICAL_DEPTH_STEP;
 	bool scattering = false, reflection = false;
-	Event accepted = after;
-	double s0 = 0.0, s1 = 0.0;
-	if(interior_interval(before, after, r_before, r_after, s0, s1))
+	Event accepted = c.after;
+	if(c.interior)
 	{
 		// Build_Optical_Depth_Pieces, src/Simulation_Trajectory.cpp:347-414
 		const int pieces = capture_mode ? DMS_CAPTURE_OPTICAL_DEPTH_PIECES : DMS_MAX_OPTICAL_DEPTH_PIECES;
-		const bool use_cached = r_before < DMS_RSUN_KM && s0 <= 1.0e-12;
-		const double span = s1 - s0;
-		double fr[DMS_MAX_OPTICAL_DEPTH_PIECES + 1], rt[DMS_MAX_OPTICAL_DEPTH_PIECES + 1];
-		bool invalid = false;
-		double dtau = 0.0, tau2 = 0.0;
-		if(s1 > s0 && actual_dt > 0.0)
-		{
-			// One loop over the piece boundaries (one copy of the rate lookup); the trapezoid
-			// sums are formed as the rates arrive, in the reference's order.  The arrays keep
-			// the boundaries for the scattering-point search, which is rare.
-			double fr_prev = 0.0, rt_prev = 0.0, fr_0 = 0.0, rt_0 = 0.0, fr_2 = 0.0, rt_2 = 0.0, tau2_a = 0.0;
-#pragma unroll 1
-			for(int i = 0; i <= pieces; i++)
-			{
-				const double f = s0 + static_cast<double>(i) / static_cast<double>(pieces) * span;
-				const double rate = (i == 0 && use_cached) ? rate_before : rate_at_fraction(S, P, before, after, f);
-				fr[i] = f;
-				rt[i] = rate;
-				if(!isfinite(rate) || rate < 0.0)
-					invalid = true;
-				if(i > 0 && f > fr_prev)
-					dtau += 0.5 * (rt_prev + rate) * (actual_dt * (f - fr_prev));
-				if(pieces >= 4)
-				{
-					// two-piece estimate over [0, 2] and [2, 4]
-					if(i == 0)
-					{
-						fr_0 = f;
-						rt_0 = rate;
-					}
-					else if(i == 2)
-					{
-						fr_2 = f;
-						rt_2 = rate;
-						tau2_a = 0.5 * (rt_0 + rt_2) * (actual_dt * (fr_2 - fr_0));
-					}
-					else if(i == 4)
-						tau2 = tau2_a + 0.5 * (rt_2 + rate) * (actual_dt * (f - fr_2));
-				}
-				else if(i > 0)
-					tau2 += 0.5 * (rt_prev + rate) * (actual_dt * (f - fr_prev));
-				fr_prev = f;
-				rt_prev = rate;
-			}
-		}
 		if(invalid || !isfinite(dtau) || dtau < 0.0)
 		{
-			set_final(L, after, true, DMS_REASON_NUMERICAL_FAILURE);
+			set_final(L, c.after, true, DMS_REASON_NUMERICAL_FAILURE);
 			return PH_FINAL;
 		}
 		const double scale = dtau > DMS_OPTICAL_DEPTH_ABS_TOL ? dtau : DMS_OPTICAL_DEPTH_ABS_TOL;
@@ -258,7 +271,7 @@ __device__ __forceinline__ int free_step_finish(const RunParams& R, const DevPoi
 			L.retries++;
 			if(L.retries > DMS_MAX_OPTICAL_DEPTH_RETRIES)
 			{
-				set_final(L, before, true, DMS_REASON_NUMERICAL_FAILURE);
+				set_final(L, c.before, true, DMS_REASON_NUMERICAL_FAILURE);
 				return PH_FINAL;
 			}
 			L.pr.time = L.b_time;
@@ -273,7 +286,7 @@ __device__ __forceinline__ int free_step_finish(const RunParams& R, const DevPoi
 				factor = 0.8 * sqrt(DMS_OPTICAL_DEPTH_REL_TOL / rel);
 			if(factor > 1.0) factor = 1.0;
 			if(factor < DMS_RK45_MIN_STEP_FACTOR) factor = DMS_RK45_MIN_STEP_FACTOR;
-			L.pr.time_step = sanitized_step(factor * actual_dt);
+			L.pr.time_step = sanitized_step(factor * c.actual_dt);
 			return PH_STEP;  // L.before still describes the restored propagator
 		}
 		if(dtau >= L.tau)
@@ -283,13 +296,13 @@ __device__ __forceinline__ int free_step_finish(const RunParams& R, const DevPoi
 			{
 				if(!(fr[k + 1] > fr[k]))
 					continue;
-				const double pdt = actual_dt * (fr[k + 1] - fr[k]);
+				const double pdt = c.actual_dt * (fr[k + 1] - fr[k]);
 				const double ptau = 0.5 * (rt[k] + rt[k + 1]) * pdt;
 				if(ptau >= remaining)
 				{
 					const double lf = solve_linear_rate(rt[k], rt[k + 1], pdt, remaining);
 					const double f = fr[k] + lf * (fr[k + 1] - fr[k]);
-					accepted = interpolate_event(before, after, f);
+					accepted = interpolate_event(c.before, c.after, f);
 					scattering = true;
 					break;
 				}
@@ -297,7 +310,7 @@ __device__ __forceinline__ int free_step_finish(const RunParams& R, const DevPoi
 			}
 			if(!scattering)
 			{
-				accepted = interpolate_event(before, after, s1);
+				accepted = interpolate_event(c.before, c.after, c.s1);
 				scattering = true;
 			}
 		}
@@ -306,21 +319,21 @@ __device__ __forceinline__ int free_step_finish(const RunParams& R, const DevPoi
 	}
 	if(!scattering)
 	{
-		Event boundary_ev = after;
-		double r_b = r_after, v_b = v_after;
-		if(r_before < R.boundary && r_after >= R.boundary && r_after > r_before)
+		Event boundary_ev = c.after;
+		double r_b = c.r_after, v_b = c.v_after;
+		if(c.r_before < R.boundary && c.r_after >= R.boundary && c.r_after > c.r_before)
 		{
-			const double f = (R.boundary - r_before) / (r_after - r_before);
-			boundary_ev = interpolate_event(before, after, f);
+			const double f = (R.boundary - c.r_before) / (c.r_after - c.r_before);
+			boundary_ev = interpolate_event(c.before, c.after, f);
 			r_b = ev_radius(boundary_ev);
 			v_b = ev_speed(boundary_ev);
 		}
-		if(r_b >= R.boundary && r_b >= r_before && v_b > solar_vesc(S, r_b))
+		if(r_b >= R.boundary && r_b >= c.r_before && v_b > solar_vesc(S, r_b))
 		{
 			accepted = boundary_ev;
 			reflection = true;
 		}
-		else if(r_b >= R.boundary && r_b >= r_before)
+		else if(r_b >= R.boundary && r_b >= c.r_before)
 		{
 			Event abs_b = boundary_ev;
 			abs_b.t += L.origin;
@@ -382,8 +395,193 @@ __device__ __forceinline__ int free_step_finish(const RunParams& R, const DevPoi
 		}
 		return PH_SCATTER;  // Sample_Target runs warp-cooperatively in the lane loop
 	}
-	L.before = after;
+	L.before = c.after;
+	// the propagator is left as the attempt made it: the next step starts from its speed and rate
+	L.next_valid = next_ok ? 1 : 0;
+	L.next_speed = c.v_after;
+	L.next_rate = next_rate;
 	return PH_STEP;
+}
+
+// A finished step on one lane: the piece rates one after another (one copy of the lookup).
+__device__ __forceinline__ int free_step_finish(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L,
+                                                double2* hist, int rk)
+{
+	const DevSolar& S = R.S;
+	const int capture_mode = R.capture_mode;
+	FinishCtx c;
+	const int ph = free_step_finish_head(R, L, rk, c);
+	if(ph != PH_CONTINUE)
+		return ph;
+	const int pieces = capture_mode ? DMS_CAPTURE_OPTICAL_DEPTH_PIECES : DMS_MAX_OPTICAL_DEPTH_PIECES;
+	const bool use_cached = c.r_before < DMS_RSUN_KM && c.s0 <= 1.0e-12;
+	const double span = c.s1 - c.s0;
+	double fr[DMS_MAX_OPTICAL_DEPTH_PIECES + 1], rt[DMS_MAX_OPTICAL_DEPTH_PIECES + 1];
+	bool invalid = false;
+	double dtau = 0.0, tau2 = 0.0;
+	if(c.depth)
+	{
+		// One loop over the piece boundaries (one copy of the rate lookup); the trapezoid
+		// sums are formed as the rates arrive, in the reference's order.  The arrays keep
+		// the boundaries for the scattering-point search, which is rare.
+		double fr_prev = 0.0, rt_prev = 0.0, fr_0 = 0.0, rt_0 = 0.0, fr_2 = 0.0, rt_2 = 0.0, tau2_a = 0.0;
+#pragma unroll 1
+		for(int i = 0; i <= pieces; i++)
+		{
+			const double f = c.s0 + static_cast<double>(i) / static_cast<double>(pieces) * span;
+			const double rate = (i == 0 && use_cached) ? c.rate_before : rate_at_fraction(S, P, c.before, c.after, f);
+			fr[i] = f;
+			rt[i] = rate;
+			if(!isfinite(rate) || rate < 0.0)
+				invalid = true;
+			if(i > 0 && f > fr_prev)
+				dtau += 0.5 * (rt_prev + rate) * (c.actual_dt * (f - fr_prev));
+			if(pieces >= 4)
+			{
+				// two-piece estimate over [0, 2] and [2, 4]
+				if(i == 0)
+				{
+					fr_0 = f;
+					rt_0 = rate;
+				}
+				else if(i == 2)
+				{
+					fr_2 = f;
+					rt_2 = rate;
+					tau2_a = 0.5 * (rt_0 + rt_2) * (c.actual_dt * (fr_2 - fr_0));
+				}
+				else if(i == 4)
+					tau2 = tau2_a + 0.5 * (rt_2 + rate) * (c.actual_dt * (f - fr_2));
+			}
+			else if(i > 0)
+				tau2 += 0.5 * (rt_prev + rate) * (c.actual_dt * (f - fr_prev));
+			fr_prev = f;
+			rt_prev = rate;
+		}
+	}
+	return free_step_finish_tail(R, m_dm, L, hist, c, fr, rt, dtau, tau2, invalid, false, 0.0);
+}
+
+// One piece-boundary rate of a step (rate_at_fraction at fraction f) or, for the job `next`, the
+// scattering rate at the propagator's state after the step (rate_total at ra, va, as the next
+// step's head forms it when ra is inside the Sun); the two share the code path, so that the lanes
+// of a warp that form them run converged.
+__device__ __forceinline__ double depth_job_rate(const DevSolar& S, const DevPoint* __restrict__ P, const Event& a, const Event& b, double f,
+                                                 bool next, double ra, double va)
+{
+	f = clamp_unit(f);
+	const double x = a.x.x + f * (b.x.x - a.x.x), vx = a.v.x + f * (b.v.x - a.v.x);
+	const double y = a.x.y + f * (b.x.y - a.x.y), vy = a.v.y + f * (b.v.y - a.v.y);
+	const double z = a.x.z + f * (b.x.z - a.x.z), vz = a.v.z + f * (b.v.z - a.v.z);
+	double r2 = 0.0, v2 = 0.0;
+	r2 += x * x;
+	v2 += vx * vx;
+	r2 += y * y;
+	v2 += vy * vy;
+	r2 += z * z;
+	v2 += vz * vz;
+	double r = sqrt(r2 > 0.0 ? r2 : 0.0), v = sqrt(v2 > 0.0 ? v2 : 0.0);
+	if(next)
+	{
+		r = ra;
+		v = va;
+	}
+	if(r >= DMS_RSUN_KM)
+		return 0.0;
+	return rate_total(S, P, r, v);
+}
+
+__device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+
+// The piece rates of every lane of the warp in `dm` (the lanes whose finished step needs them),
+// formed by the whole warp at once: job j of a step (j = 0..PIECES, the boundaries; PIECES + 1,
+// the next step's rate) runs on its own lane with the step's events broadcast from its owner,
+// in as many rounds of 32 jobs as the steps need.  Each lookup is the function and arguments of
+// the one-lane loop, so the rates are the same numbers.  Every lane of the warp calls this.
+template <int PIECES>
+__device__ __forceinline__ void coop_depth_rates(const RunParams& R, const DevPoint* __restrict__ P, const FinishCtx& c, bool depth,
+                                                 unsigned int dm, double (&fr)[DMS_MAX_OPTICAL_DEPTH_PIECES + 1],
+                                                 double (&rt)[DMS_MAX_OPTICAL_DEPTH_PIECES + 1], double& next_rate)
+{
+	constexpr int J = PIECES + 2;
+	const int me = threadIdx.x & 31;
+	const int jobs = __popc(dm) * J;
+	const int rank = __popc(dm & ((1u << me) - 1u));  // among the lanes of dm (when depth)
+	const double span = c.s1 - c.s0;
+	for(int base = 0; base < jobs; base += 32)
+	{
+		const int job = base + me;
+		const bool active = job < jobs;
+		const int oi = active ? job / J : 0;
+		const int j = active ? job - oi * J : 0;
+		const int owner = nth_set_bit(dm, oi);
+		Event a, b;
+		a.x = mk(shfl_d(c.before.x.x, owner), shfl_d(c.before.x.y, owner), shfl_d(c.before.x.z, owner));
+		a.v = mk(shfl_d(c.before.v.x, owner), shfl_d(c.before.v.y, owner), shfl_d(c.before.v.z, owner));
+		b.x = mk(shfl_d(c.after.x.x, owner), shfl_d(c.after.x.y, owner), shfl_d(c.after.x.z, owner));
+		b.v = mk(shfl_d(c.after.v.x, owner), shfl_d(c.after.v.y, owner), shfl_d(c.after.v.z, owner));
+		const double s0 = shfl_d(c.s0, owner), sp = shfl_d(span, owner);
+		const double ra = shfl_d(c.r_after, owner), va = shfl_d(c.v_after, owner);
+		const DevPoint* Po = reinterpret_cast<const DevPoint*>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(P), owner));
+		double rate = 0.0;
+		if(active)
+			rate = depth_job_rate(R.S, Po, a, b, s0 + static_cast<double>(j) / static_cast<double>(PIECES) * sp, j == J - 1, ra, va);
+#pragma unroll
+		for(int jj = 0; jj < J; jj++)
+		{
+			const int src = rank * J + jj - base;
+			const bool here = depth && src >= 0 && src < 32;
+			const double v = shfl_d(rate, here ? src : me);
+			if(here)
+			{
+				if(jj < J - 1)
+					rt[jj] = v;
+				else
+					next_rate = v;
+			}
+		}
+	}
+	if(depth)
+	{
+#pragma unroll
+		for(int i = 0; i <= PIECES; i++)
+			fr[i] = c.s0 + static_cast<double>(i) / static_cast<double>(PIECES) * span;
+		if(c.r_before < DMS_RSUN_KM && c.s0 <= 1.0e-12)
+			rt[0] = c.rate_before;
+	}
+}
+
+// A finished step on every lane of the warp that holds one (want), the piece rates formed by the
+// whole warp (coop_depth_rates).  Every lane of the warp calls this; the others only help.
+__device__ __forceinline__ int free_step_finish_warp(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L,
+                                                     double2* hist, int rk, bool want)
+{
+	FinishCtx c = {};
+	int ph = PH_STEP;
+	if(want)
+		ph = free_step_finish_head(R, L, rk, c);
+	const bool depth = want && ph == PH_CONTINUE && c.depth;
+	const unsigned int dm = __ballot_sync(0xffffffffu, depth);
+	double fr[DMS_MAX_OPTICAL_DEPTH_PIECES + 1], rt[DMS_MAX_OPTICAL_DEPTH_PIECES + 1];
+	double next_rate = 0.0, dtau = 0.0, tau2 = 0.0;
+	bool invalid = false;
+	if(dm != 0u)
+	{
+		if(R.capture_mode)
+			coop_depth_rates<DMS_CAPTURE_OPTICAL_DEPTH_PIECES>(R, P, c, depth, dm, fr, rt, next_rate);
+		else
+			coop_depth_rates<DMS_MAX_OPTICAL_DEPTH_PIECES>(R, P, c, depth, dm, fr, rt, next_rate);
+	}
+	if(depth)
+	{
+		if(R.capture_mode)
+			depth_sums<DMS_CAPTURE_OPTICAL_DEPTH_PIECES>(fr, rt, c.actual_dt, dtau, tau2, invalid);
+		else
+			depth_sums<DMS_MAX_OPTICAL_DEPTH_PIECES>(fr, rt, c.actual_dt, dtau, tau2, invalid);
+	}
+	if(want && ph == PH_CONTINUE)
+		return free_step_finish_tail(R, m_dm, L, hist, c, fr, rt, dtau, tau2, invalid, depth, next_rate);
+	return ph;
 }
 
 // Initial_Conditions + Hyperbolic_Kepler_Shift of every work index (src/Data_Generation.cpp:747-761,
@@ -443,6 +641,12 @@ struct StrictStep
 	                                      int rk) const
 	{
 		return free_step_finish(R, P, m_dm, L, hist, rk);
+	}
+	// the finish of the paired attempts: all lanes of the warp call this (want: the lane's own)
+	__device__ __forceinline__ int finish_warp(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L, double2* hist,
+	                                           int rk, bool want) const
+	{
+		return free_step_finish_warp(R, P, m_dm, L, hist, rk, want);
 	}
 	__device__ __forceinline__ int operator()(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, StrictLane& L, double2* hist,
 	                                          int drained) const

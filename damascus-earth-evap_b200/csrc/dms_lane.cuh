@@ -48,6 +48,8 @@ struct LaneT
 	int in_rk;           // an RK45 step is in progress (retry pending)
 	int rk_inner;        // passes of the current RK45 step
 	double rate_before;  // scattering rate at the start of the step
+	int next_valid;      // next_speed / next_rate hold the propagator's speed and rate (FP64 form, tail)
+	double next_speed, next_rate;
 	double b_time, b_radius, b_phi, b_vr, b_step;  // propagator fields at the start of the step
 	int shift_ok;
 	int reason;
@@ -221,6 +223,7 @@ __device__ __forceinline__ int segment_start(const RunParams& R, const DevPoint*
 	L.seg_steps = 0;
 	L.retries = 0;
 	L.before_valid = 0;
+	L.next_valid = 0;
 	L.in_rk = 0;
 	if(!R.capture_mode && L.prev_time >= 0.0)
 		L.prev_time = 0.0;
@@ -797,8 +800,10 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 					}
 				}
 				const int rk = step.pair_attempt(R.S, L, role, partner);
+				// the finished steps' piece rates are formed by the whole warp
+				const int ph = step.finish_warp(R, P, m_dm, L, hist, rk, want);
 				if(want)
-					phase = step.finish(R, P, m_dm, L, hist, rk);
+					phase = ph;
 			}
 			else if(want)
 				phase = step.finish(R, P, m_dm, L, hist, step.attempt(R.S, L, drained));
