@@ -46,10 +46,10 @@ WORKLOAD = ("Parameter-point evaporation (config 1): SI contact m=0.3 GeV sigma_
 # conditions, Kepler shift, classification).
 FLOP_PER_ATTEMPT, FLOP_PER_STEP, FLOP_PER_SCATTER, FLOP_PER_TRAJ = 214.8, 622.3, 2455.0, 3374.0
 # DRAM bytes (read + write) of the FP64 trajectory kernel per trajectory of this point, from one
-# ncu capture of one 65 536-trajectory batch (ids 0-65 535: 2.684 GB read + 4.939 GB written, 512
+# ncu capture of one 65 536-trajectory batch (ids 0-65 535: 2.671 GB read + 6.777 GB written, 635
 # bytes per accepted step): the lane state's local-memory traffic and the termination flush of
 # the per-lane histogram rows.
-TRAFFIC_PER_TRAJECTORY = (2.684434e9 + 4.939171e9) / 65536
+TRAFFIC_PER_TRAJECTORY = (2.671374e9 + 6.777167e9) / 65536
 
 
 def hbm_peak_gbs():
