@@ -986,7 +986,7 @@ __device__ __forceinline__ int rk45_attempt_pair(const DevSolar& S, Prop& p, int
 	const double R = q.radius, V = q.v_radial;
 	double a, b;
 	const double kr0 = dt * V;
-	// round 1: stage 0 (owner) | stage 1 (helper)
+	// first pair: stage 0 (owner) | stage 1 (helper)
 	const double r_s1 = R + kr0 / 4.0;
 	cert_stage<true>(S, q, odd ? r_s1 : R, a, b, good);
 	const double kv_m1 = dt * a, kp_m1 = dt * b;
@@ -994,7 +994,7 @@ __device__ __forceinline__ int rk45_attempt_pair(const DevSolar& S, Prop& p, int
 	const double kv0 = odd ? kv_o1 : kv_m1, kv1 = odd ? kv_m1 : kv_o1;
 	const double kr1 = dt * (V + kv0 / 4.0);
 	const double kr2 = dt * (V + 3.0 / 32.0 * kv0 + 9.0 / 32.0 * kv1);
-	// round 2: stage 2 | stage 3
+	// second pair: stage 2 | stage 3
 	const double r_s2 = R + 3.0 / 32.0 * kr0 + 9.0 / 32.0 * kr1;
 	const double r_s3 = R + 1932.0 / 2197.0 * kr0 - 7200.0 / 2197.0 * kr1 + 7296.0 / 2197.0 * kr2;
 	cert_stage<true>(S, q, odd ? r_s3 : r_s2, a, b, good);
@@ -1003,7 +1003,7 @@ __device__ __forceinline__ int rk45_attempt_pair(const DevSolar& S, Prop& p, int
 	const double kv2 = odd ? kv_o2 : kv_m2, kv3 = odd ? kv_m2 : kv_o2;
 	const double kr3 = dt * (V + 1932.0 / 2197.0 * kv0 - 7200.0 / 2197.0 * kv1 + 7296.0 / 2197.0 * kv2);
 	const double kr4 = dt * (V + 439.0 / 216.0 * kv0 - 8.0 * kv1 + 3680.0 / 513.0 * kv2 - 845.0 / 4104.0 * kv3);
-	// round 3: stage 4 | stage 5
+	// third pair: stage 4 | stage 5
 	const double r_s4 = R + 439.0 / 216.0 * kr0 - 8.0 * kr1 + 3680.0 / 513.0 * kr2 - 845.0 / 4104.0 * kr3;
 	const double r_s5 = R - 8.0 / 27.0 * kr0 + 2.0 * kr1 - 3544.0 / 2565.0 * kr2 + 1859.0 / 4104.0 * kr3 - 11.0 / 40.0 * kr4;
 	cert_stage<true>(S, q, odd ? r_s5 : r_s4, a, b, good);
