@@ -613,6 +613,70 @@ __global__ void __launch_bounds__(128) initial_state_kernel(const RunParams R)
 	R.init[w] = st;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Tail pipeline.  A lane that runs alone spends its step on one dependent chain, and the
+// divergent paths of a warp do not overlap, but two warps do.  So once a block has drained, a
+// warp whose lanes are all done stays as the block's helper: a stepping lane (the owner) hands it
+// its propagator through shared memory, the helper makes the step's head (free_step_begin) and
+// its RK45 attempts (paired on its lanes 0 and 1), and the owner adopts the result.  Right after
+// adopting, the owner hands over the next step's start, computed as if the step it is about to
+// finish ends plainly (the propagator unchanged, one more free step), and finishes the step
+// meanwhile.  It adopts that speculative result only when its state is then bit for bit the one
+// the speculation started from; otherwise it discards it and hands over its actual state.  The
+// helper runs the same functions on the same values, so the results are the same.  One owner per
+// block; every wait is bounded by the global timer, and a wait that runs out detaches the owner,
+// which then steps on its own.
+enum PipeState : int
+{
+	PIPE_NONE = 0,      // no helper
+	PIPE_FREE = 1,      // a helper waits for an owner
+	PIPE_ATTACHED = 2,
+	PIPE_CLOSED = 3,
+};
+
+struct PipeBox
+{
+	int state, job, done;  // job / done: sequence numbers of the hand-over and of its result
+	int begin_phase, rk, rk_inner;
+	const DevPoint* P;
+	uint64_t seg_in;
+	Prop pr_in, pr_out;
+	Event before_out;
+	double b_time, b_radius, b_phi, b_vr, b_step, rate_before;
+};
+
+__device__ __forceinline__ PipeBox& pipe_box()
+{
+	__shared__ PipeBox box;
+	return box;
+}
+
+// bounds of the waits, in SM clock cycles (about 2 GHz)
+constexpr long long PIPE_WAIT_CYCLES = 2000000ll;            // an owner's wait for a result (~1 ms, 100 steps)
+constexpr long long PIPE_IDLE_FREE_CYCLES = 400000ll;        // a helper without owner leaves after ~0.2 ms
+constexpr long long PIPE_IDLE_ATTACHED_CYCLES = 10000000ll;  // ~5 ms (an owner hands over every step)
+
+__device__ __forceinline__ bool pipe_wait(const PipeBox& b, int seq)
+{
+	const long long t0 = clock64();
+	while(*reinterpret_cast<const volatile int*>(&b.done) != seq)
+	{
+		if(clock64() - t0 > PIPE_WAIT_CYCLES)
+			return false;
+		__nanosleep(32);  // leaves the issue slots to the other warps of the SM
+	}
+	__threadfence_block();
+	return true;
+}
+
+__device__ __forceinline__ bool same_prop(const Prop& a, const Prop& b)
+{
+	auto eq = [](double x, double y) { return __double_as_longlong(x) == __double_as_longlong(y); };
+	return eq(a.time, b.time) && eq(a.radius, b.radius) && eq(a.phi, b.phi) && eq(a.v_radial, b.v_radial) && eq(a.J, b.J) &&
+	       eq(a.time_step, b.time_step) && eq(a.ax.x, b.ax.x) && eq(a.ax.y, b.ax.y) && eq(a.ax.z, b.ax.z) && eq(a.ay.x, b.ay.x) &&
+	       eq(a.ay.y, b.ay.y) && eq(a.ay.z, b.ay.z) && a.radial_mode == b.radial_mode;
+}
+
 struct StrictStep
 {
 	// the lane loop runs a step as begin / attempt / finish and may pair the attempt of a lane
@@ -663,6 +727,179 @@ struct StrictStep
 	__device__ __forceinline__ bool scatter(const DevSolar& S, const DevPoint* __restrict__ P, Draws& D, Event& e, int target) const
 	{
 		return scatter_with_target(S, P, D, e, target);
+	}
+
+	// ---- tail pipeline (see PipeBox) ----
+	static constexpr bool pipeline = DMS_TAIL_PIPELINE != 0 && pairs;
+	__device__ __forceinline__ void pipe_init() const
+	{
+		PipeBox& b = pipe_box();
+		b.state = PIPE_NONE;
+		b.job = 0;
+		b.done = 0;
+	}
+	// all lanes of a warp whose lanes are all done call this; it returns when the warp leaves
+	// (it was not needed as the helper, or it has served its last owner)
+	__device__ void pipe_serve(const RunParams& R, StrictLane& L) const
+	{
+		PipeBox& b = pipe_box();
+		const int me = threadIdx.x & 31;
+		int became = 0;
+		if(me == 0)
+			became = atomicCAS(&b.state, PIPE_NONE, PIPE_FREE) == PIPE_NONE ? 1 : 0;
+		if(__shfl_sync(0xffffffffu, became, 0) == 0)
+			return;
+		// a helper that served before this one left every hand-over answered (done == job)
+		int last = __shfl_sync(0xffffffffu, *reinterpret_cast<volatile int*>(&b.job), 0);
+		long long idle_since = clock64();
+		for(unsigned int poll = 0;; poll++)
+		{
+			const int job = __shfl_sync(0xffffffffu, *reinterpret_cast<volatile int*>(&b.job), 0);
+			if(job != last)
+			{
+				__threadfence_block();
+				pipe_job(R, L, b);
+				__threadfence_block();
+				if(me == 0)
+					*reinterpret_cast<volatile int*>(&b.done) = job;
+				last = job;
+				idle_since = clock64();
+				continue;
+			}
+			const int st = __shfl_sync(0xffffffffu, *reinterpret_cast<volatile int*>(&b.state), 0);
+			const long long idle = clock64() - idle_since;
+			// the cancel flag lives in host memory: read it rarely
+			const bool cancelled = (poll & 4095u) == 4095u && __any_sync(0xffffffffu, *R.cancel != 0);
+			if(cancelled || (st == PIPE_FREE && idle > PIPE_IDLE_FREE_CYCLES) || (st != PIPE_FREE && idle > PIPE_IDLE_ATTACHED_CYCLES))
+			{
+				int closed = 1;
+				if(me == 0)
+				{
+					// without an owner the box is left for a warp that is done later; an owner may
+					// attach meanwhile, and then the helper stays
+					if(st == PIPE_FREE && !cancelled)
+						closed = atomicCAS(&b.state, PIPE_FREE, PIPE_NONE) == PIPE_FREE ? 1 : 0;
+					else
+						atomicExch(&b.state, PIPE_CLOSED);
+				}
+				if(__shfl_sync(0xffffffffu, closed, 0))
+					return;
+				continue;
+			}
+			__nanosleep(64);
+		}
+	}
+	// the helper's work for one hand-over: the step's head on lane 0 (its own lane state as
+	// scratch), then the RK45 attempts paired on lanes 0 and 1 until one is not retried
+	__device__ __forceinline__ void pipe_job(const RunParams& R, StrictLane& L, PipeBox& b) const
+	{
+		const int me = threadIdx.x & 31;
+		int ph = PH_STEP;
+		if(me == 0)
+		{
+			L.pr = b.pr_in;
+			L.seg_steps = b.seg_in;
+			L.before_valid = 0;  // the head forms Event_In_3D of the propagator (= the owner's cached one)
+			L.next_valid = 0;
+			L.in_rk = 0;
+			ph = free_step_begin(R, b.P, L);
+		}
+		ph = __shfl_sync(0xffffffffu, ph, 0);
+		int rk = RK_RETRY, passes = 0;
+		if(ph == PH_STEP)
+		{
+			const int role = me == 0 ? 1 : (me == 1 ? 2 : 0);
+			const int partner = me == 0 ? 1 : 0;
+			while(rk == RK_RETRY && passes <= DMS_RK45_MAX_INNER_RETRIES + 1)
+			{
+				rk = __shfl_sync(0xffffffffu, pair_attempt(R.S, L, role, partner), 0);
+				passes++;
+			}
+		}
+		if(me == 0)
+		{
+			b.begin_phase = (ph == PH_STEP && rk == RK_RETRY) ? PH_FINAL : ph;  // a step that never ended: the owner steps alone
+			b.rk = rk;
+			b.rk_inner = L.rk_inner;
+			b.pr_out = L.pr;
+			b.before_out = L.before;
+			b.b_time = L.b_time;
+			b.b_radius = L.b_radius;
+			b.b_phi = L.b_phi;
+			b.b_vr = L.b_vr;
+			b.b_step = L.b_step;
+			b.rate_before = L.rate_before;
+		}
+	}
+	__device__ __forceinline__ bool pipe_attach() const
+	{
+		PipeBox& b = pipe_box();
+		return *reinterpret_cast<volatile int*>(&b.state) == PIPE_FREE && atomicCAS(&b.state, PIPE_FREE, PIPE_ATTACHED) == PIPE_FREE;
+	}
+	__device__ __forceinline__ int pipe_post(const DevPoint* __restrict__ P, const Prop& pr, uint64_t seg) const
+	{
+		PipeBox& b = pipe_box();
+		b.P = P;
+		b.pr_in = pr;
+		b.seg_in = seg;
+		__threadfence_block();
+		const int seq = b.job + 1;
+		*reinterpret_cast<volatile int*>(&b.job) = seq;
+		return seq;
+	}
+	__device__ __forceinline__ void pipe_adopt(const PipeBox& b, StrictLane& L) const
+	{
+		L.pr = b.pr_out;
+		L.before = b.before_out;
+		L.before_valid = 1;
+		L.next_valid = 0;
+		L.b_time = b.b_time;
+		L.b_radius = b.b_radius;
+		L.b_phi = b.b_phi;
+		L.b_vr = b.b_vr;
+		L.b_step = b.b_step;
+		L.rate_before = b.rate_before;
+		L.in_rk = 1;
+		L.rk_inner = b.rk_inner;
+	}
+	// the owner's step start: 1 = adopted (rk set), 0 = make the head here, -1 = detached
+	__device__ __forceinline__ int pipe_step(const DevPoint* __restrict__ P, StrictLane& L, int& spec, int& rk) const
+	{
+		PipeBox& b = pipe_box();
+		if(*reinterpret_cast<volatile int*>(&b.state) != PIPE_ATTACHED)
+		{
+			spec = 0;
+			return -1;  // the helper has left
+		}
+		if(spec != 0)
+		{
+			const int s = spec;
+			spec = 0;
+			if(!pipe_wait(b, s))
+				return -1;
+			if(b.begin_phase == PH_STEP && b.P == P && b.seg_in == L.seg_steps && same_prop(b.pr_in, L.pr))
+			{
+				pipe_adopt(b, L);
+				rk = b.rk;
+				return 1;
+			}
+		}
+		const int s = pipe_post(P, L.pr, L.seg_steps);
+		if(!pipe_wait(b, s))
+			return -1;
+		if(b.begin_phase != PH_STEP)
+			return 0;
+		pipe_adopt(b, L);
+		rk = b.rk;
+		return 1;
+	}
+	__device__ __forceinline__ void pipe_release(int& spec) const
+	{
+		PipeBox& b = pipe_box();
+		if(spec != 0)
+			pipe_wait(b, spec);
+		spec = 0;
+		atomicCAS(&b.state, PIPE_ATTACHED, PIPE_FREE);
 	}
 };
 

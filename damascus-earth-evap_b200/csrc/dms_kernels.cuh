@@ -42,6 +42,11 @@
 #ifndef DMS_RK_UNROLLED_MIXED
 #define DMS_RK_UNROLLED_MIXED 1
 #endif
+// The FP64 tail pipeline (a second warp of a drained block makes a lone lane's step head and
+// attempts while the lane finishes its previous step) when 1.
+#ifndef DMS_TAIL_PIPELINE
+#define DMS_TAIL_PIPELINE 1
+#endif
 #ifndef DMS_TRAJ_MIN_BLOCKS_MIXED
 #define DMS_TRAJ_MIN_BLOCKS_MIXED 4
 #endif

@@ -364,6 +364,7 @@ __device__ __forceinline__ int free_step_mixed(const RunParams& R, const DevPoin
 struct MixedStep
 {
 	static constexpr bool pairs = false;
+	static constexpr bool pipeline = false;
 	__device__ __forceinline__ int operator()(const RunParams& R, const DevPoint* __restrict__ P, double m_dm, MixedLane& L, double2* hist,
 	                                          int drained) const
 	{

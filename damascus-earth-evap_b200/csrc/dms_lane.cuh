@@ -688,6 +688,9 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	__shared__ int queue_drained;
 	if(threadIdx.x == 0)
 		queue_drained = 0;
+	if constexpr(Step::pipeline)
+		if(threadIdx.x == 0)
+			step.pipe_init();
 	__syncthreads();
 	Lane L;
 	FlushJob job;
@@ -701,6 +704,10 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	// the lane's claimed ids [q_next, q_end): R.queue_chunk ids per claim
 	uint64_t q_next = 0, q_end = 0;
 	const unsigned int lane_bit = 1u << (threadIdx.x & 31);
+	// tail pipeline: this lane owns the block's helper warp; pipe_spec is the hand-over of the
+	// next step's start made before the current finish (0 = none)
+	bool pipe_owner = false;
+	int pipe_spec = 0;
 	// Every lane stays in the loop until its whole warp is done (a lane without work waits in
 	// PH_DONE), and leaves only together with the others.  So the warp's collective steps
 	// below (batching votes, cooperative target sampling into the warp's shared rates, the
@@ -710,7 +717,12 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 	for(uint64_t iter = 0;; iter++)
 	{
 		if(__all_sync(FULL_WARP, phase == PH_DONE))
+		{
+			if constexpr(Step::pipeline)
+				if(R.wall_limit_ns == 0 && blockDim.x > 32)
+					step.pipe_serve(R, L);  // the warp may stay as the block's helper
 			break;
+		}
 #if DMS_RK_UNROLLED == 2 || DMS_RK_UNROLLED_MIXED == 2
 		// a block whose lanes are all held by long trajectories learns of the drained queue from
 		// the queue head itself (one read per warp every 64 iterations)
@@ -771,42 +783,82 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 			// chain of a lane that runs alone, the tail of a launch.  Same results either way.
 			const int drained = *reinterpret_cast<volatile int*>(&queue_drained);
 			bool want = false;
+			bool piped = false;  // the step's head and attempts came from the helper warp
+			int rk_piped = RK_RETRY;
+			if constexpr(Step::pipeline)
+			{
+				// only a lane that steps alone in its warp owns the helper: an owner's waits hold its
+				// whole warp.  An owner that ends its trajectory or stops being alone releases it.
+				const unsigned int stepping = __ballot_sync(FULL_WARP, phase == PH_STEP);
+				const bool alone = phase == PH_STEP && stepping == lane_bit;
+				if(pipe_owner && !alone && phase != PH_SCATTER && phase != PH_SEGMENT)
+				{
+					step.pipe_release(pipe_spec);
+					pipe_owner = false;
+				}
+				if(alone && !L.in_rk && drained && R.wall_limit_ns == 0)
+				{
+					if(!pipe_owner)
+						pipe_owner = step.pipe_attach();
+					if(pipe_owner)
+					{
+						const int r = step.pipe_step(P, L, pipe_spec, rk_piped);
+						piped = r == 1;
+						if(r < 0)
+							pipe_owner = false;  // the helper did not answer: step alone
+					}
+				}
+			}
 			if(phase == PH_STEP)
 			{
-				const int ph = step.begin(R, P, L);
-				want = ph == PH_STEP;
-				if(!want)
-					phase = ph;
+				if(piped)
+					want = true;
+				else
+				{
+					const int ph = step.begin(R, P, L);
+					want = ph == PH_STEP;
+					if(!want)
+						phase = ph;
+				}
 			}
-			const unsigned int att = __ballot_sync(FULL_WARP, want);
+			if constexpr(Step::pipeline)
+			{
+				// hand over the next step's start now, so that it is made during this finish
+				if(piped && rk_piped == RK_ACCEPTED)
+					pipe_spec = step.pipe_post(P, L.pr, L.seg_steps + 1);
+			}
+			const unsigned int att = __ballot_sync(FULL_WARP, want && !piped);
+			const unsigned int busy = __ballot_sync(FULL_WARP, want);
 			const int n_att = __popc(att);
-			if(n_att != 0 && n_att <= DMS_PAIR_MAX_LANES && (drained || !DMS_PAIR_ONLY_DRAINED))
+			// every attempting lane needs an idle lane (a piped lane is busy without attempting)
+			if(busy != 0u && n_att <= DMS_PAIR_MAX_LANES && n_att + __popc(busy) <= 32 && (drained || !DMS_PAIR_ONLY_DRAINED))
 			{
 				const int me = threadIdx.x & 31;
 				int role = 0, partner = me;
 				const unsigned int below = lane_bit - 1u;
-				if(want)
+				if(want && !piped)
 				{
 					role = 1;
-					partner = nth_set_bit(~att, __popc(att & below));
+					partner = nth_set_bit(~busy, __popc(att & below));
 				}
-				else
+				else if(!want)
 				{
-					const int q = __popc(~att & below);
+					const int q = __popc(~busy & below);
 					if(q < n_att)
 					{
 						role = 2;
 						partner = nth_set_bit(att, q);
 					}
 				}
-				const int rk = step.pair_attempt(R.S, L, role, partner);
+				// (a warp whose only busy lane was piped has no attempt to make)
+				const int rk = n_att != 0 ? step.pair_attempt(R.S, L, role, partner) : RK_RETRY;
 				// the finished steps' piece rates are formed by the whole warp
-				const int ph = step.finish_warp(R, P, m_dm, L, hist, rk, want);
+				const int ph = step.finish_warp(R, P, m_dm, L, hist, piped ? rk_piped : rk, want);
 				if(want)
 					phase = ph;
 			}
 			else if(want)
-				phase = step.finish(R, P, m_dm, L, hist, step.attempt(R.S, L, drained));
+				phase = step.finish(R, P, m_dm, L, hist, piped ? rk_piped : step.attempt(R.S, L, drained));
 		}
 		else if(phase == PH_STEP)
 			phase = step(R, P, m_dm, L, hist, *reinterpret_cast<volatile int*>(&queue_drained));
