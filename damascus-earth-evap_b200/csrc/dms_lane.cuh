@@ -780,7 +780,10 @@ __device__ __forceinline__ void lane_loop(const RunParams& R, Step step)
 			// A step is opened per lane; its RK45 attempt then runs paired when at most half of
 			// the warp is attempting: every attempting lane takes an idle lane of its warp as a
 			// helper for the independent stages (rk45_attempt_pair), which shortens the dependent
-			// chain of a lane that runs alone, the tail of a launch.  Same results either way.
+			// chain of a lane that runs alone, the tail of a launch.  Same results either way.  With
+			// Step::pipeline a lane that steps alone in its warp may instead hand its step head and
+			// attempts to the block's helper warp (see PipeBox); such a lane is busy ("piped")
+			// without attempting here.
 			const int drained = *reinterpret_cast<volatile int*>(&queue_drained);
 			bool want = false;
 			bool piped = false;  // the step's head and attempts came from the helper warp
